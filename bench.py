@@ -1,0 +1,340 @@
+"""pyr3-b200 benchmark: chaos-game iterations/s on one of the seeded
+workloads (default: the headline 1080p, 12-xform + final configuration).
+
+A step is one full frame of the hot path: reset (zero the histogram),
+iterate (all quality x W x H post-fuse samples), present (density estimation
+when the workload sets it, tonemap to RGBA8).  `value` is the device time of
+the K timed steps (CUDA events on the renderer's stream, L2 flushed between
+steps, inputs already resident); `e2e` is the same metric through the public
+API with the palette / genome uploaded and the image read back every step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--impl reference]
+
+With --gpus N > 1 (launched by torchrun) every rank renders an independent
+replica of the workload (the path has no exchange step: replicas only) and
+rank 0 reports N x samples / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "headline": ("iters/s (1080p, 12 xforms)", "headline_1080p"),
+    "plain_small": ("iters/s (640x480, 3 xforms)", "plain_small"),
+    "motion_4k": ("iters/s (4K, 6 xforms, 8 temporal samples)", "motion_4k"),
+}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    def __init__(self, device: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={device}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap,utilization.gpu",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                util = float(f[6])
+                if util < 50:
+                    continue
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[2 + k].lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _workload(name):
+    from pyr3_b200 import workloads
+
+    g = getattr(workloads, CONFIGS[name][1])()
+    if isinstance(g, tuple):  # motion blur: shutter-open keyframe drives the bench
+        g = g[0]
+    return g
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        return ws, rank, local, dist
+    return 1, 0, 0, None
+
+
+def _max_over_ranks(x: float, dist, local: int) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# --------------------------------------------------------------- CPU baseline
+def cpu_reference_rate(g, target_seconds: float = 12.0, threads: int | None = None):
+    """The reference's own chaos loop (its WGSL compiled for the CPU,
+    oracle/_ref) on the host cores: a bounded sample of the workload
+    (1024 walkers, the reference's TARGET_WALKERS, x fewer iterations)."""
+    from oracle import oracle as O
+    from pyr3_b200 import genome as G
+
+    threads = threads or os.cpu_count() or 1
+    ge = G.expand_for_gpu(g)
+    xf = G.pack_xforms(ge)
+    pal = G.bake_lut(ge.palette, ge.palette_hue, ge.palette_interp)
+    w = np.array([x.weight for x in ge.xforms], np.float64)
+    xa = G.xaos_matrix(ge)
+    distrib = O.pack_xform_distrib(w, None if xa is None else xa.astype(np.float64))
+    W, H = g.size
+    os_ = g.oversample
+    walkers = 1024
+
+    def run(iters):
+        u = np.zeros(31, np.uint32)
+        f = u.view(np.float32)
+        i32 = u.view(np.int32)
+        u[0], u[1], u[2], u[3] = W * os_, H * os_, iters, 200
+        f[4], f[5], f[6] = g.scale * os_, g.cx, g.cy
+        u[7] = 1
+        i32[8] = G.final_slot(ge)
+        f[9] = np.float32(g.rotate * np.pi / 180.0)
+        u[10] = 1 if g.palette_mode == "linear" else 0
+        u[12] = walkers
+        f[13] = 1e-7
+        f[30] = g.xform_blend
+        hist = np.zeros(W * os_ * H * os_ * 4, np.uint32)
+        isaac = O.pack_isaac_states(walkers, 1)
+        t0 = time.perf_counter()
+        O.ref_chaos_run(u, xf, len(ge.xforms), pal, distrib, isaac, 0, walkers, hist, threads)
+        return time.perf_counter() - t0
+
+    probe_iters = 256
+    dt = run(probe_iters)
+    rate = walkers * (probe_iters + 200) / max(dt, 1e-6)
+    iters = int(max(256, min(2_000_000, rate * target_seconds / walkers - 200)))
+    dt = run(iters)
+    samples = walkers * iters  # post-fuse samples
+    return samples / dt, threads, f"{walkers} walkers x {iters} iterations (+200 fuse) of the workload genome"
+
+
+# ------------------------------------------------------------------ ours
+def bench_ours(args, ws, rank, local, dist):
+    from pyr3_b200 import _lib, renderer as R
+
+    g = _workload(args.config)
+    W, H = g.size
+    os_ = g.oversample
+    walkers, iters, samples = R.compute_dispatch(g.quality, W, H)
+    r = R.create_renderer(W, H, os_, g.filter_radius, device=local)
+    gg = R.GpuGenome(g)
+    r.prepare(gg)  # NVRTC specialisation (cached), outside the timed region
+    lib = _lib.lib()
+    h = r.handle
+    p = r.present_opts(g)
+    out_dev = None
+    import torch  # device buffer for the present output
+
+    out_dev = torch.empty((H, W, 4), dtype=torch.uint8, device=f"cuda:{local}")
+    pal = None
+    from pyr3_b200.genome import bake_lut
+
+    pal = bake_lut(g.palette, g.palette_hue, g.palette_interp)
+    L2_FLUSH = 256 << 20
+
+    def step_device(seed):
+        _lib.check(lib.pyr3_reset(h, _lib.ptr(pal)))
+        r.iterate(gg, seed, walkers, iters)
+        _lib.check(lib.pyr3_present_device(h, C.byref(p), samples, C.c_void_p(out_dev.data_ptr()),
+                                           _lib.OUT_RGBA8))
+
+    for k in range(args.warmup):
+        step_device(1000 + k)
+    r.sync()
+    _barrier(dist)
+    clocks = Clocks(local) if rank == 0 else None
+    total_ms, chaos_ms = 0.0, []
+    for k in range(args.steps):
+        _lib.check(lib.pyr3_flush_l2(h, L2_FLUSH))
+        _lib.check(lib.pyr3_mark(h, 0))
+        step_device(k)
+        _lib.check(lib.pyr3_mark(h, 1))
+        ms = C.c_float()
+        _lib.check(lib.pyr3_elapsed(h, 0, 1, C.byref(ms)))
+        total_ms += ms.value
+        chaos_ms.append(r.last_iterate_ms())
+    clk = clocks.stop() if clocks else None
+    n_samples, n_splats = r.counters()
+    _barrier(dist)
+    t_max = _max_over_ranks(total_ms, dist, local)
+
+    # e2e through the public API: host palette + genome in, RGBA8 image out
+    host_img = np.zeros((H, W, 4), np.uint8)
+    for k in range(max(1, args.warmup // 2)):
+        r.reset(g)
+        r.iterate(g, 5000 + k, walkers, iters)
+        r.present(g, samples, out=host_img)
+    e2e_ms = 0.0
+    for k in range(args.steps):
+        _lib.check(lib.pyr3_flush_l2(h, L2_FLUSH))
+        _lib.check(lib.pyr3_mark(h, 2))
+        r.reset(g)
+        r.iterate(g, 7000 + k, walkers, iters)
+        r.present(g, samples, out=host_img)
+        _lib.check(lib.pyr3_mark(h, 3))
+        ms = C.c_float()
+        _lib.check(lib.pyr3_elapsed(h, 2, 3, C.byref(ms)))
+        e2e_ms += ms.value
+    e2e_max = _max_over_ranks(e2e_ms, dist, local)
+
+    if rank != 0:
+        r.destroy()
+        return None
+    value = ws * samples * args.steps / (t_max / 1e3)
+    e2e = ws * samples * args.steps / (e2e_max / 1e3)
+    peak, peak_kind = _peaks()
+    # Dominant kernel: the chaos kernel.  Algorithmic bytes per launch: every
+    # in-canvas splat reads and writes one 16-byte RGBA u32 bucket.
+    splats_per_launch = n_splats / max(1, (args.steps + args.warmup + max(1, args.warmup // 2)))
+    mean_chaos = statistics.mean(chaos_ms)
+    achieved = splats_per_launch * 32.0 / (mean_chaos / 1e3) / 1e9
+    h2d = 4096 + gg.xforms.nbytes + (len(g.xforms) + 1) * len(g.xforms) * 2
+    line = {
+        "metric": CONFIGS[args.config][0], "value": value, "unit": "iters/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded genome, pyr3_b200/workloads.py)",
+        "config": {"workload": args.config, "canvas": [W, H], "oversample": os_,
+                   "quality_spp": g.quality, "samples_per_step": samples,
+                   "xforms": len(g.xforms), "final_xform": g.finalxform is not None,
+                   "density_estimation": g.density is not None,
+                   "l2": "256 MiB scratch overwritten between timed steps",
+                   "parallelism": f"replicas x{ws}"},
+        "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(host_img.nbytes)},
+        "chaos_kernel_ms": mean_chaos,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "note": f"chaos kernel; algorithmic bytes = 32 B (16 B bucket read+write) per "
+                             f"in-canvas splat; peak {peak_kind}"},
+        "gpu_launches": args.steps * (2 + (1 if g.density is not None else 0)),
+        "clocks": clk,
+    }
+    if ws == 1 and not args.no_cpu_baseline:
+        rate, cores, sample = cpu_reference_rate(g)
+        line["cpu_baseline"] = {"value": rate, "unit": "iters/s", "cores": cores, "kind": "reference",
+                                "sample": sample}
+    r.destroy()
+    return line
+
+
+def bench_reference(args, ws, rank, local, dist):
+    if rank != 0:
+        return None
+    g = _workload(args.config)
+    per = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_reference_rate(g, target_seconds=per)
+    rates = []
+    sample = ""
+    cores = 0
+    for _ in range(args.steps):
+        rate, cores, sample = cpu_reference_rate(g, target_seconds=per)
+        rates.append(rate)
+    value = statistics.mean(rates)
+    return {"impl": "reference", "metric": CONFIGS[args.config][0], "value": value, "unit": "iters/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.config},
+            "cpu_baseline": {"value": value, "unit": "iters/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="headline", choices=sorted(CONFIGS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    ws, rank, local, dist = _dist()
+    try:
+        line = bench_reference(args, ws, rank, local, dist) if args.impl == "reference" else \
+            bench_ours(args, ws, rank, local, dist)
+        if line is not None:
+            print(json.dumps(line))
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

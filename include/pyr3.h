@@ -1,0 +1,204 @@
+/*
+ * pyr3-b200 C-ABI: the drop-in boundary that replaces the reference's
+ * WebGPU passes under its Renderer API (MattAltermatt/pyr3
+ * src/renderer.ts:163-318).  Plain pointers and sizes only; every function
+ * returns 0 on success or a negative PYR3_E* code, with a message available
+ * from pyr3_last_error().
+ *
+ * Threading: one renderer handle per host thread.  Work is enqueued on the
+ * renderer's CUDA stream and is asynchronous until pyr3_sync() or a call
+ * that returns host data (pyr3_read_histogram, pyr3_present to a host
+ * buffer, pyr3_counters).
+ *
+ * Buffers: the caller owns every host buffer it passes; the renderer owns
+ * all device memory it allocates (recreated on pyr3_resize).  Entries that
+ * take DEVICE pointers say so.
+ */
+#ifndef PYR3_H
+#define PYR3_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PYR3_OK 0
+#define PYR3_E_INVALID (-1)   /* bad argument / malformed genome */
+#define PYR3_E_CUDA (-2)      /* CUDA runtime or driver error */
+#define PYR3_E_NVRTC (-3)     /* JIT compile of the chaos kernel failed */
+#define PYR3_E_NOMEM (-4)     /* device allocation failed */
+#define PYR3_E_UNSUPPORTED (-5) /* variation index not in this build */
+
+#define PYR3_XFORM_FLOATS 116  /* packed xform record (src/genome.ts:293-313) */
+#define PYR3_MAX_XFORMS 128    /* src/genome.ts:326 */
+#define PYR3_PALETTE_FLOATS 1024 /* 256 x RGBA f32 (src/palette.ts:211) */
+
+typedef struct pyr3_renderer pyr3_renderer;
+
+/* createRenderer options (src/renderer.ts:78-86). */
+typedef struct {
+  uint32_t width, height; /* output canvas */
+  uint32_t oversample;    /* >= 1; super-res canvas = width*os x height*os */
+  float filter_radius;    /* spatial filter radius in output px; <= 0 -> 0.5 */
+  int32_t device;         /* CUDA device ordinal */
+} pyr3_opts;
+
+/* A genome as the reference's chaos pass receives it after
+ * expandGenomeForGPU (src/symmetry.ts:21) and packXforms
+ * (src/genome.ts:408): n_xforms regular records followed, when
+ * final_slot >= 0, by the final xform record at slot n_xforms. */
+typedef struct {
+  const float *xforms;    /* (n_xforms + (final_slot >= 0)) x 116 f32 */
+  uint32_t n_xforms;      /* 1..128 */
+  int32_t final_slot;     /* -1 or n_xforms (src/genome.ts:432) */
+  const float *xaos;      /* n_xforms x n_xforms row-major or NULL */
+  float scale, cx, cy;    /* viewport (pixels per unit at output res) */
+  float rotate_deg;       /* CCW camera rotation */
+  uint32_t palette_mode;  /* 0 step (flam3 default), 1 linear */
+  float xform_blend;      /* 0..1 (chaos.wgsl:8372) */
+} pyr3_genome;
+
+/* iterate() request (src/renderer.ts:127-146 + chaos.ts:381-456). */
+typedef struct {
+  uint64_t walkers;        /* reference walker count for this chunk */
+  uint64_t iters_per_walker;
+  uint32_t seed;
+  float walker_jitter;     /* < 0 -> default 1e-7 */
+  uint32_t color_mode;     /* 0 palette, 1 flow, 2 trap, 3 phase */
+  float flow_strength, flow_scale;
+  uint32_t trap_kind, trap_mode;
+  float trap_cx, trap_cy, trap_radius, trap_angle_deg, trap_falloff, trap_freq, trap_strength;
+  float phase_strength, phase_freq;
+  uint32_t flags;          /* PYR3_ITER_* */
+} pyr3_iterate_opts;
+
+/* Use exactly `walkers` ISAAC streams x `iters_per_walker` iterations, as
+ * the reference dispatch does.  Without it the renderer keeps the sample
+ * total walkers*iters but spreads it over its own persistent walker pool
+ * (each stream still seeded by the reference's packIsaacStates rule). */
+#define PYR3_ITER_EXACT_WALKERS 1u
+/* Warp-aggregate identical histogram buckets with __match_any_sync. */
+#define PYR3_ITER_AGGREGATE 2u
+
+/* present() request (src/renderer.ts:148-158, visualize.ts:178-204). */
+typedef struct {
+  float gamma, vibrancy, highpow, brightness, linrange; /* src/tonemap.ts */
+  int32_t density_on;       /* 1 -> density estimation pass */
+  float de_max_rad, de_min_rad, de_curve;               /* src/density.ts */
+  float background[3];
+  int32_t transparent;
+  double scale;             /* genome.scale (calibration k2) */
+} pyr3_present_opts;
+
+#define PYR3_OUT_RGBA8 0      /* W x H x 4 u8 (rgba8unorm) */
+#define PYR3_OUT_RGBA32F 1    /* W x H x 4 f32 (fragment value) */
+
+/* ---- lifecycle -------------------------------------------------------- */
+/* createRenderer (src/renderer.ts:214). */
+int pyr3_create(const pyr3_opts *opts, pyr3_renderer **out);
+/* Renderer.destroy (src/renderer.ts:316). */
+int pyr3_destroy(pyr3_renderer *r);
+/* Renderer.resize (src/renderer.ts:281). */
+int pyr3_resize(pyr3_renderer *r, const pyr3_opts *opts);
+/* Last error message of the calling thread ("" if none). */
+const char *pyr3_last_error(void);
+
+/* ---- the render path -------------------------------------------------- */
+/* Renderer.reset (src/renderer.ts:221): upload the palette (256 x RGBA f32,
+ * the bakeLUT output of src/palette.ts:71) and zero the histogram. */
+int pyr3_reset(pyr3_renderer *r, const float *palette);
+/* Renderer.iterate (src/renderer.ts:227) -> chaos.dispatch
+ * (src/chaos.ts:333): accumulate walkers*iters post-fuse samples. */
+int pyr3_iterate(pyr3_renderer *r, const pyr3_genome *g, const pyr3_iterate_opts *o);
+/* Renderer.present (src/renderer.ts:241): density estimation (optional) +
+ * tonemap of the accumulated histogram.  total_samples = sum of
+ * walkers*iters since reset.  `out` is a HOST buffer of W*H*4 u8 or f32
+ * per out_kind; the call returns after the copy. */
+int pyr3_present(pyr3_renderer *r, const pyr3_present_opts *p, uint64_t total_samples,
+                 void *out, int32_t out_kind);
+/* Same as pyr3_present but writes into a DEVICE buffer and returns without
+ * synchronising. */
+int pyr3_present_device(pyr3_renderer *r, const pyr3_present_opts *p, uint64_t total_samples,
+                        void *device_out, int32_t out_kind);
+/* Renderer.readHistogram (src/renderer.ts:209, src/chaos.ts:293): raw
+ * super-res histogram, superW*superH*4 u32 (R, G, B, count). */
+int pyr3_read_histogram(pyr3_renderer *r, uint32_t *host_out);
+/* Renderer.readIndexMap (src/renderer.ts:205): superW*superH u32 colour
+ * index sums (valid after iterating with capture on). */
+int pyr3_read_index_map(pyr3_renderer *r, uint32_t *host_out);
+/* Renderer.setCaptureIndex (src/renderer.ts:200). */
+int pyr3_set_capture_index(pyr3_renderer *r, int32_t on);
+/* Wait for all work queued on the renderer. */
+int pyr3_sync(pyr3_renderer *r);
+/* Super-res dimensions and device histogram pointer (for callers that keep
+ * data on the GPU). */
+int pyr3_info(pyr3_renderer *r, uint32_t *super_w, uint32_t *super_h, void **device_hist);
+/* Accepted post-fuse samples and in-canvas splats since reset. */
+int pyr3_counters(pyr3_renderer *r, uint64_t *samples, uint64_t *splats);
+/* Device time in ms of the last pyr3_iterate chaos launch (CUDA events). */
+int pyr3_last_iterate_ms(pyr3_renderer *r, float *ms);
+
+/* CUDA-event timing on the renderer's stream: record mark `slot` (0..7),
+ * then read the device time between two marks (waits for the later one). */
+int pyr3_mark(pyr3_renderer *r, int32_t slot);
+int pyr3_elapsed(pyr3_renderer *r, int32_t a, int32_t b, float *ms);
+/* Overwrite a scratch buffer of `bytes` on the renderer's stream (evicts
+ * the L2 between timed steps). */
+int pyr3_flush_l2(pyr3_renderer *r, uint64_t bytes);
+
+/* ---- stage entry points (parity tests and tools) ---------------------- */
+/* packIsaacStates (src/isaac.ts:194) computed on the device: n x 36 u32 in
+ * the reference layout for walkers base..base+n-1. */
+int pyr3_seed_walkers(uint32_t seed, uint64_t base, uint32_t n, uint32_t *host_out);
+/* Evaluate one variation (apply_variation, chaos.wgsl:7731) on n points on
+ * the device; isaac (n x 36 u32, reference layout) is each point's RNG
+ * stream and is updated in place. params10/a0/a1 as in the packed xform. */
+int pyr3_eval_variation(uint32_t idx, uint32_t n, const float *pts_xy, float weight,
+                        const float *params10, const float *a0, const float *a1,
+                        uint32_t *isaac, float *out_xy);
+/* Direct colour of a DC variation (dc_color_for, chaos.wgsl:8192) at n
+ * points; hit[i] = 1 when the variation colours the point. */
+int pyr3_eval_dc_color(uint32_t idx, uint32_t n, const float *pts_xy, const float *v4,
+                       const float *ve4, float *out_rgb, int32_t *hit);
+/* Xform pick of an explicit draw stream (chaos.wgsl:8343): prev[i] < 0
+ * selects the no-prior row.  weights / xaos as in pyr3_genome. */
+int pyr3_pick_stream(uint32_t n_xforms, const float *weights, const float *xaos,
+                     uint32_t count, const int32_t *prev, const uint32_t *draws,
+                     uint32_t *out);
+/* Splat an explicit point stream (x, y, colour, opacity per point) into a
+ * zeroed width x height x 4 u32 histogram with the chaos kernel's
+ * saturating scatter (chaos.wgsl:8567-8718, colour mode 0). */
+int pyr3_splat_points(uint32_t n, const float *pts, uint32_t width, uint32_t height,
+                      float scale, float cx, float cy, float rotation_rad,
+                      uint32_t palette_mode, const float *palette, int32_t aggregate,
+                      uint32_t *hist_inout);
+/* Density estimation + tonemap of a given super-res histogram (no chaos
+ * pass): out = width x height x RGBA f32. */
+int pyr3_density_tonemap(const uint32_t *hist, uint32_t width, uint32_t height,
+                         uint32_t oversample, float filter_radius, const pyr3_present_opts *p,
+                         uint64_t total_samples, float *out_rgba, float *filtered_out);
+/* Compile (or fetch from cache) the chaos kernel for a genome structure;
+ * returns the NVRTC log on failure via pyr3_last_error. */
+int pyr3_prepare(pyr3_renderer *r, const pyr3_genome *g);
+
+/* ---- build checks (no GPU needed) ------------------------------------ */
+/* Generate + NVRTC-compile the chaos kernel for a genome structure without
+ * touching a device; *cubin_bytes receives the image size. */
+int pyr3_jit_compile(const pyr3_genome *g, int32_t aggregate, uint64_t *cubin_bytes);
+/* Copy the generated NVRTC source for a genome into buf (size cap); returns
+ * the full length through *len. */
+int pyr3_jit_source(const pyr3_genome *g, char *buf, uint64_t cap, uint64_t *len);
+/* NVRTC-compile the variation evaluator for `idx` (no device). */
+int pyr3_jit_compile_variation(uint32_t idx, uint64_t *cubin_bytes);
+/* The (n+1) x 16384 xform pick table (src/genome.ts:482-534; row n = the
+ * no-prior row) as the renderer reproduces it from its per-row boundaries. */
+int pyr3_pick_table(uint32_t n_xforms, const float *weights, const float *xaos,
+                    uint32_t *table_out);
+/* 1 if this build implements variation idx, 0 if not; name via *name. */
+int pyr3_variation_info(uint32_t idx, int32_t *implemented, int32_t *is_dc, const char **name);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYR3_H */

@@ -1,0 +1,98 @@
+"""Build libpyr3cuda.so in-tree (sm_100a).
+
+1. Embed the NVRTC sources (csrc/jit/*.cuh) and the variation table
+   (catalog.json names; which variations / direct colours the library
+   implements, found by scanning the VAR(...) / DCV(...) definitions) into
+   csrc/gen/jit_sources.inc.
+2. nvcc -gencode arch=compute_100a,code=sm_100a the C-ABI (capi.cpp), the
+   JIT driver (jit.cpp) and the density / tonemap passes (passes.cu).
+"""
+from __future__ import annotations
+
+import glob
+import json
+import os
+import re
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+JIT = os.path.join(CSRC, "jit")
+GEN = os.path.join(CSRC, "gen")
+LIB = os.path.join(PKG, "libpyr3cuda.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CUDA_LIB = "/usr/local/cuda/lib64"
+
+
+def _strip(src: str) -> str:
+    return "\n".join(l for l in src.splitlines() if l.strip() != "#pragma once")
+
+
+def _raw(s: str) -> str:
+    # Raw string literals, split so no single literal gets unwieldy.
+    parts = []
+    chunk = 60000
+    for i in range(0, len(s), chunk):
+        parts.append('R"PYR3SRC(' + s[i:i + chunk] + ')PYR3SRC"')
+    return "\n".join(parts) if parts else '""'
+
+
+def generate_sources() -> str:
+    os.makedirs(GEN, exist_ok=True)
+    core = _strip(open(os.path.join(JIT, "vlib_core.cuh")).read())
+    vlibs = sorted(f for f in glob.glob(os.path.join(JIT, "vlib_*.cuh")) if not f.endswith("vlib_core.cuh"))
+    vsrc = [_strip(open(f).read()) for f in vlibs]
+    chaos = _strip(open(os.path.join(JIT, "chaos_kernel.cuh")).read())
+    marker = "// ==== PYR3 KERNEL SECTION ===="
+    pre, kern = chaos.split(marker, 1)
+    ev = _strip(open(os.path.join(JIT, "eval_kernel.cuh")).read())
+    cat = json.load(open(os.path.join(PKG, "catalog.json")))["variations"]
+    names = [v["name"] for v in cat]
+    allsrc = "\n".join(vsrc)
+    impl = set(re.findall(r"^VAR\((\w+)\)", allsrc, re.M))
+    dcs = set(re.findall(r"^DCV\((\w+)\)", allsrc, re.M))
+    unknown = (impl | dcs) - set(names)
+    if unknown:
+        raise RuntimeError(f"variation library defines names not in the catalog: {sorted(unknown)}")
+    out = ["// generated by pyr3_b200/build.py -- do not edit"]
+    out.append(f"static const char* const kSrcCore = {_raw(core)};")
+    out.append(f"static const int kNumVlib = {len(vsrc)};")
+    out.append("static const char* const kSrcVlib[] = {" + ",\n".join(_raw(s) for s in vsrc) + "};")
+    out.append(f"static const char* const kSrcChaosPre = {_raw(pre)};")
+    out.append(f"static const char* const kSrcChaosKernel = {_raw(kern)};")
+    out.append(f"static const char* const kSrcEval = {_raw(ev)};")
+    out.append("static const char* const kVarNames[326] = {" + ", ".join(f'"{n}"' for n in names) + "};")
+    out.append("static const unsigned char kVarImpl[326] = {" +
+               ", ".join("1" if n in impl else "0" for n in names) + "};")
+    out.append("static const unsigned char kVarDc[326] = {" +
+               ", ".join("1" if n in dcs else "0" for n in names) + "};")
+    text = "\n".join(out) + "\n"
+    path = os.path.join(GEN, "jit_sources.inc")
+    if not os.path.exists(path) or open(path).read() != text:
+        with open(path, "w") as f:
+            f.write(text)
+    return path
+
+
+def build(force: bool = False) -> str:
+    inc = generate_sources()
+    srcs = [os.path.join(CSRC, f) for f in ("capi.cpp", "jit.cpp", "passes.cu")]
+    deps = srcs + [inc, os.path.join(ROOT, "include", "pyr3.h"), os.path.join(CSRC, "jit.h"),
+                   os.path.join(CSRC, "passes.h")]
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
+        return LIB
+    cmd = [NVCC, "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+           "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared",
+           "-I", os.path.join(ROOT, "include"), "-I", CSRC, *srcs, "-o", LIB,
+           "-cudart", "static", "-L", CUDA_LIB, "-lnvrtc",
+           "-Xlinker", f"-rpath,{CUDA_LIB}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv))

@@ -1,0 +1,864 @@
+// pyr3-b200 C-ABI (include/pyr3.h): renderer lifecycle, the iterate /
+// present path, and stage entry points for parity tests.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "jit.h"
+#include "passes.h"
+#include "pyr3.h"
+
+#define PYR3_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                            \
+  do {                                                                            \
+    cudaError_t e_ = (expr);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(e_ == cudaErrorMemoryAllocation ? PYR3_E_NOMEM : PYR3_E_CUDA,   \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));            \
+  } while (0)
+
+// Launch a kernel of a JIT-loaded library (cudaKernel_t).
+#define LAUNCH_TRY(kernel, grid, block, smem, stream, args)                       \
+  CUDA_TRY(cudaLaunchKernel((const void*)(kernel), dim3(grid), dim3(block), args, smem, stream))
+
+constexpr uint32_t kGrain = 16384;
+constexpr uint32_t kFuse = 200;         // src/renderer.ts:41
+constexpr float kDefaultJitter = 1e-7f; // src/chaos.ts:96
+constexpr int kWpb = 256;
+
+// Host mirror of the NVRTC kernel's argument block (layout must match
+// ChaosArgs in csrc/jit/chaos_kernel.cuh).
+struct ChaosArgs {
+  uint32_t* hist;
+  uint32_t* idx_sum;
+  const float* palette;
+  const unsigned short* pick_start;
+  uint64_t walker_base, n_walkers, iters_base, iters_extra;
+  uint32_t fuse;
+  uint32_t width, height;
+  float scale, cx, cy;
+  float cos_r, sin_r;
+  uint32_t seed;
+  float jitter;
+  uint32_t palette_mode;
+  uint32_t capture_index;
+  uint32_t color_mode;
+  float flow_strength, flow_scale;
+  uint32_t trap_kind, trap_mode;
+  float trap_cx, trap_cy, trap_radius, trap_nx, trap_ny, trap_falloff, trap_freq, trap_strength;
+  float phase_strength, phase_freq;
+  float xform_blend;
+  uint64_t* counters;
+};
+
+// ---- host restatements of the reference's host-side math --------------
+// Pick table (src/genome.ts:482-534) as per-row boundaries: start[r][j] is
+// the first grain index whose table entry is >= j, so the device recovers
+// the 16384-entry table exactly (see pick_xform in chaos_kernel.cuh).
+bool build_pick_starts(int n, const float* weights_f, const float* xaos, std::vector<uint16_t>* out,
+                       std::string* err) {
+  std::vector<double> w(n);
+  for (int i = 0; i < n; ++i) w[i] = (double)weights_f[i];
+  out->assign((size_t)(n + 1) * n, (uint16_t)kGrain);
+  std::vector<uint32_t> row(kGrain);
+  for (int r = 0; r <= n; ++r) {
+    const int xi = r < n ? r : -1;
+    auto mult = [&](int j) -> double {
+      return (xi >= 0 && xaos && j < n) ? (double)xaos[(size_t)xi * n + j] : 1.0;
+    };
+    double sum = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double d = w[i] * mult(i);
+      if (!std::isfinite(d) || d < 0) {
+        *err = "xform weight must be non-negative finite";
+        return false;
+      }
+      sum += d;
+    }
+    std::fill(row.begin(), row.end(), 0u);
+    if (sum != 0.0) {
+      const double dr = sum / kGrain;
+      int j = 0;
+      double t = w[0] * mult(0), acc = 0.0;
+      for (uint32_t g = 0; g < kGrain; ++g) {
+        while (acc >= t && j <= n) {
+          ++j;
+          t += (j < n ? w[j] : 0.0) * mult(j);
+        }
+        row[g] = (uint32_t)std::min(j, n - 1);
+        acc += dr;
+      }
+    }
+    uint16_t* st = out->data() + (size_t)r * n;
+    st[0] = 0;
+    for (int j = 1; j < n; ++j) {
+      uint32_t g = 0;
+      while (g < kGrain && row[g] < (uint32_t)j) ++g;
+      st[j] = (uint16_t)g;
+    }
+  }
+  return true;
+}
+
+// src/density.ts:78-99.
+void kernel_norm_lut(float* out) {
+  for (int r = 0; r <= 256; ++r) {
+    if (r == 0) {
+      out[0] = 1.0f;
+      continue;
+    }
+    const double sigma = r / 3.0, inv2s2 = 1.0 / (2.0 * sigma * sigma), r2 = (double)r * r;
+    double sum = 0.0;
+    for (int dy = -r; dy <= r; ++dy)
+      for (int dx = -r; dx <= r; ++dx) {
+        const double d2 = (double)dx * dx + (double)dy * dy;
+        if (d2 <= r2) sum += std::exp(-d2 * inv2s2);
+      }
+    out[r] = (float)sum;
+  }
+}
+
+// src/spatial-filter.ts:217-256 (gaussian shape).
+int spatial_kernel(double radius, int os, float* out) {
+  const double supp = 1.5;
+  const double fw = 2.0 * supp * os * radius;
+  int fwidth = (int)std::floor(fw) + 1;
+  if (((fwidth ^ os) & 1) != 0) fwidth++;
+  fwidth = std::max(3, std::min(pyr3::kMaxTaps, fwidth));
+  const double adjust = fw > 0 ? (supp * fwidth) / fw : 1.0;
+  double v[pyr3::kMaxTaps], sum = 0.0;
+  for (int i = 0; i < fwidth; ++i) {
+    const double x = ((2.0 * i + 1.0) / fwidth - 1.0) * adjust;
+    v[i] = std::exp(-2.0 * x * x);
+    sum += v[i];
+  }
+  for (int i = 0; i < fwidth; ++i) {
+    const float tap = (float)v[i];
+    out[i] = sum != 0 ? (float)((double)tap / sum) : tap;
+  }
+  return fwidth;
+}
+
+int g_num_sms = 0;
+
+int device_sms(int dev) {
+  if (g_num_sms == 0) cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+  return g_num_sms > 0 ? g_num_sms : 148;
+}
+
+}  // namespace
+
+struct pyr3_renderer {
+  int device = 0;
+  uint32_t W = 0, H = 0, os = 1, SW = 0, SH = 0;
+  float filter_radius = 0.5f;
+  int fwidth = 3;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  uint32_t* d_hist = nullptr;
+  uint32_t* d_idx = nullptr;
+  float* d_filtered = nullptr;
+  float* d_pal = nullptr;
+  float* d_knorm = nullptr;
+  float* d_kwtab = nullptr;
+  float* d_kern = nullptr;
+  void* d_out = nullptr;
+  size_t out_bytes = 0;
+  uint16_t* d_pick = nullptr;
+  size_t pick_cap = 0;
+  uint64_t* d_counters = nullptr;
+  bool capture = false;
+  float last_ms = 0.0f;
+  cudaEvent_t marks[8] = {};
+  void* d_flush = nullptr;
+  size_t flush_bytes = 0;
+  std::vector<std::shared_ptr<pyr3::ChaosModule>> modules;  // keep-alive
+};
+
+namespace {
+
+void free_buffers(pyr3_renderer* r) {
+  cudaFree(r->d_hist);
+  cudaFree(r->d_idx);
+  cudaFree(r->d_filtered);
+  cudaFree(r->d_out);
+  r->d_hist = r->d_idx = nullptr;
+  r->d_filtered = nullptr;
+  r->d_out = nullptr;
+  r->out_bytes = 0;
+}
+
+int alloc_buffers(pyr3_renderer* r, const pyr3_opts* o) {
+  if (!o || o->width == 0 || o->height == 0 || o->oversample == 0)
+    return fail(PYR3_E_INVALID, "width, height and oversample must be positive");
+  if ((uint64_t)o->width * o->oversample > 65535 || (uint64_t)o->height * o->oversample > 65535)
+    return fail(PYR3_E_INVALID, "super-res canvas exceeds 65535 pixels per side");
+  r->W = o->width;
+  r->H = o->height;
+  r->os = o->oversample;
+  r->SW = r->W * r->os;
+  r->SH = r->H * r->os;
+  r->filter_radius = o->filter_radius > 0 ? o->filter_radius : 0.5f;
+  float kern[pyr3::kMaxTaps];
+  r->fwidth = spatial_kernel(r->filter_radius, (int)r->os, kern);
+  const size_t n = (size_t)r->SW * r->SH;
+  CUDA_TRY(cudaMalloc(&r->d_hist, n * 16));
+  CUDA_TRY(cudaMalloc(&r->d_idx, n * 4));
+  CUDA_TRY(cudaMemsetAsync(r->d_hist, 0, n * 16, r->stream));
+  CUDA_TRY(cudaMemsetAsync(r->d_idx, 0, n * 4, r->stream));
+  CUDA_TRY(cudaMemcpyAsync(r->d_kern, kern, sizeof kern, cudaMemcpyHostToDevice, r->stream));
+  return PYR3_OK;
+}
+
+int ensure_filtered(pyr3_renderer* r) {
+  if (!r->d_filtered) CUDA_TRY(cudaMalloc(&r->d_filtered, (size_t)r->SW * r->SH * 16));
+  return PYR3_OK;
+}
+
+int ensure_out(pyr3_renderer* r, size_t bytes) {
+  if (r->out_bytes < bytes) {
+    cudaFree(r->d_out);
+    r->d_out = nullptr;
+    CUDA_TRY(cudaMalloc(&r->d_out, bytes));
+    r->out_bytes = bytes;
+  }
+  return PYR3_OK;
+}
+
+int set_device(int dev) {
+  CUDA_TRY(cudaSetDevice(dev));
+  CUDA_TRY(cudaFree(nullptr));  // create / bind the primary context for the driver API
+  return PYR3_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- lifecycle
+PYR3_API const char* pyr3_last_error(void) { return g_err.c_str(); }
+
+PYR3_API int pyr3_create(const pyr3_opts* opts, pyr3_renderer** out) {
+  if (!opts || !out) return fail(PYR3_E_INVALID, "null argument");
+  int rc = set_device(opts->device);
+  if (rc) return rc;
+  std::unique_ptr<pyr3_renderer> r(new pyr3_renderer());
+  r->device = opts->device;
+  CUDA_TRY(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreate(&r->ev0));
+  CUDA_TRY(cudaEventCreate(&r->ev1));
+  CUDA_TRY(cudaMalloc(&r->d_pal, 1024 * 4));
+  CUDA_TRY(cudaMemsetAsync(r->d_pal, 0, 1024 * 4, r->stream));
+  CUDA_TRY(cudaMalloc(&r->d_knorm, 257 * 4));
+  CUDA_TRY(cudaMalloc(&r->d_kwtab, pyr3::kw_table_floats() * 4));
+  CUDA_TRY(cudaMalloc(&r->d_kern, pyr3::kMaxTaps * 4));
+  CUDA_TRY(cudaMalloc(&r->d_counters, 16));
+  CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, 16, r->stream));
+  float knorm[257];
+  kernel_norm_lut(knorm);
+  CUDA_TRY(cudaMemcpyAsync(r->d_knorm, knorm, sizeof knorm, cudaMemcpyHostToDevice, r->stream));
+  CUDA_TRY(pyr3::build_kw_table(r->d_knorm, r->d_kwtab, r->stream));
+  rc = alloc_buffers(r.get(), opts);
+  if (rc) {
+    free_buffers(r.get());
+    return rc;
+  }
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  *out = r.release();
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_destroy(pyr3_renderer* r) {
+  if (!r) return PYR3_OK;
+  cudaSetDevice(r->device);
+  if (r->stream) cudaStreamSynchronize(r->stream);
+  free_buffers(r);
+  cudaFree(r->d_pal);
+  cudaFree(r->d_knorm);
+  cudaFree(r->d_kwtab);
+  cudaFree(r->d_kern);
+  cudaFree(r->d_pick);
+  cudaFree(r->d_counters);
+  cudaFree(r->d_flush);
+  for (auto& e : r->marks)
+    if (e) cudaEventDestroy(e);
+  if (r->ev0) cudaEventDestroy(r->ev0);
+  if (r->ev1) cudaEventDestroy(r->ev1);
+  if (r->stream) cudaStreamDestroy(r->stream);
+  delete r;
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_resize(pyr3_renderer* r, const pyr3_opts* o) {
+  if (!r || !o) return fail(PYR3_E_INVALID, "null argument");
+  const float fr = o->filter_radius > 0 ? o->filter_radius : 0.5f;
+  if (o->width == r->W && o->height == r->H && o->oversample == r->os && fr == r->filter_radius)
+    return PYR3_OK;
+  int rc = set_device(r->device);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  free_buffers(r);
+  return alloc_buffers(r, o);
+}
+
+PYR3_API int pyr3_reset(pyr3_renderer* r, const float* palette) {
+  if (!r) return fail(PYR3_E_INVALID, "null renderer");
+  cudaSetDevice(r->device);
+  if (palette)
+    CUDA_TRY(cudaMemcpyAsync(r->d_pal, palette, 1024 * 4, cudaMemcpyHostToDevice, r->stream));
+  const size_t n = (size_t)r->SW * r->SH;
+  CUDA_TRY(cudaMemsetAsync(r->d_hist, 0, n * 16, r->stream));
+  CUDA_TRY(cudaMemsetAsync(r->d_idx, 0, n * 4, r->stream));
+  CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, 16, r->stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_set_capture_index(pyr3_renderer* r, int32_t on) {
+  if (!r) return fail(PYR3_E_INVALID, "null renderer");
+  r->capture = on != 0;
+  return PYR3_OK;
+}
+
+// ---------------------------------------------------------------- iterate
+static int prepare_module(pyr3_renderer* r, const pyr3_genome* g, bool aggregate,
+                          std::shared_ptr<pyr3::ChaosModule>* mod) {
+  if (!g || !g->xforms) return fail(PYR3_E_INVALID, "null genome");
+  pyr3::GenomeShape shape;
+  std::string e = pyr3::shape_from_packed(g->xforms, (int)g->n_xforms, g->final_slot, &shape);
+  if (!e.empty())
+    return fail(e.find("not implemented") != std::string::npos ? PYR3_E_UNSUPPORTED : PYR3_E_INVALID, e);
+  std::string err;
+  int rc = pyr3::get_chaos_module(shape, kWpb, aggregate, mod, &err);
+  if (rc) return fail(rc, err);
+  if (r && std::find(r->modules.begin(), r->modules.end(), *mod) == r->modules.end())
+    r->modules.push_back(*mod);
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_prepare(pyr3_renderer* r, const pyr3_genome* g) {
+  if (r) cudaSetDevice(r->device);
+  std::shared_ptr<pyr3::ChaosModule> m;
+  return prepare_module(r, g, false, &m);
+}
+
+PYR3_API int pyr3_iterate(pyr3_renderer* r, const pyr3_genome* g, const pyr3_iterate_opts* o) {
+  if (!r || !g || !o) return fail(PYR3_E_INVALID, "null argument");
+  cudaSetDevice(r->device);
+  const bool aggregate = (o->flags & PYR3_ITER_AGGREGATE) != 0;
+  std::shared_ptr<pyr3::ChaosModule> m;
+  int rc = prepare_module(r, g, aggregate, &m);
+  if (rc) return rc;
+  const int n = (int)g->n_xforms;
+  const bool has_final = g->final_slot >= 0;
+  // pick table boundaries
+  std::vector<float> weights(n);
+  for (int i = 0; i < n; ++i) weights[i] = g->xforms[(size_t)i * 116 + 3];
+  std::vector<uint16_t> starts;
+  std::string err;
+  if (!build_pick_starts(n, weights.data(), g->xaos, &starts, &err)) return fail(PYR3_E_INVALID, err);
+  const size_t pick_bytes = starts.size() * 2;
+  if (r->pick_cap < pick_bytes) {
+    CUDA_TRY(cudaStreamSynchronize(r->stream));
+    cudaFree(r->d_pick);
+    r->d_pick = nullptr;
+    CUDA_TRY(cudaMalloc(&r->d_pick, std::max<size_t>(pick_bytes, 4096)));
+    r->pick_cap = std::max<size_t>(pick_bytes, 4096);
+  }
+  CUDA_TRY(cudaMemcpyAsync(r->d_pick, starts.data(), pick_bytes, cudaMemcpyHostToDevice, r->stream));
+  const size_t xf_bytes = (size_t)(n + (has_final ? 1 : 0)) * 116 * 4;
+  if (xf_bytes > m->c_xf_bytes) return fail(PYR3_E_INVALID, "xform records exceed module constant bank");
+  CUDA_TRY(cudaMemcpyAsync(m->c_xf, g->xforms, xf_bytes, cudaMemcpyHostToDevice, r->stream));
+
+  // walker decomposition
+  const uint64_t total = o->walkers * o->iters_per_walker;
+  if (total == 0) return PYR3_OK;
+  uint64_t nw, base, extra;
+  const int sms = device_sms(r->device);
+  const uint64_t pool = (uint64_t)m->blocks_per_sm * sms * m->wpb;
+  if (o->flags & PYR3_ITER_EXACT_WALKERS) {
+    nw = o->walkers;
+    base = o->iters_per_walker;
+    extra = 0;
+  } else {
+    // Keep the sample total; use enough walkers to fill the machine, but
+    // not so many that the per-walker burn-in dominates.
+    uint64_t want = std::max<uint64_t>((uint64_t)sms * m->wpb, total / (5ull * kFuse));
+    nw = std::min<uint64_t>(pool, std::min<uint64_t>(want, total));
+    base = total / nw;
+    extra = total % nw;
+  }
+  ChaosArgs A;
+  std::memset(&A, 0, sizeof A);
+  A.hist = r->d_hist;
+  A.idx_sum = r->capture ? r->d_idx : nullptr;
+  A.palette = r->d_pal;
+  A.pick_start = r->d_pick;
+  A.walker_base = 0;
+  A.n_walkers = nw;
+  A.iters_base = base;
+  A.iters_extra = extra;
+  A.fuse = kFuse;
+  A.width = r->SW;
+  A.height = r->SH;
+  A.scale = (float)((double)g->scale * (double)r->os);
+  A.cx = g->cx;
+  A.cy = g->cy;
+  const float rot = (float)(((double)g->rotate_deg * M_PI) / 180.0);
+  A.cos_r = std::cos(rot);
+  A.sin_r = std::sin(rot);
+  A.seed = o->seed;
+  A.jitter = o->walker_jitter >= 0.0f ? o->walker_jitter : kDefaultJitter;
+  A.palette_mode = g->palette_mode;
+  A.capture_index = r->capture ? 1u : 0u;
+  A.color_mode = o->color_mode;
+  A.flow_strength = o->flow_strength;
+  A.flow_scale = o->flow_scale;
+  A.trap_kind = o->trap_kind;
+  A.trap_mode = o->trap_mode;
+  A.trap_cx = o->trap_cx;
+  A.trap_cy = o->trap_cy;
+  A.trap_radius = o->trap_radius;
+  const double ta = (double)o->trap_angle_deg * M_PI / 180.0;
+  A.trap_nx = (float)-std::sin(ta);
+  A.trap_ny = (float)std::cos(ta);
+  A.trap_falloff = o->trap_falloff;
+  A.trap_freq = o->trap_freq;
+  A.trap_strength = o->trap_strength;
+  A.phase_strength = o->phase_strength;
+  A.phase_freq = o->phase_freq;
+  A.xform_blend = std::min(1.0f, std::max(0.0f, g->xform_blend));
+  A.counters = r->d_counters;
+  const uint64_t sets = (nw + m->wpb - 1) / m->wpb;
+  const uint64_t resident = (uint64_t)m->blocks_per_sm * sms;
+  const unsigned grid = (unsigned)std::min<uint64_t>(sets, resident);
+  void* params[] = {&A};
+  CUDA_TRY(cudaEventRecord(r->ev0, r->stream));
+  LAUNCH_TRY(m->chaos, grid, (unsigned)m->wpb, m->smem, r->stream, params);
+  CUDA_TRY(cudaEventRecord(r->ev1, r->stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_last_iterate_ms(pyr3_renderer* r, float* ms) {
+  if (!r || !ms) return fail(PYR3_E_INVALID, "null argument");
+  CUDA_TRY(cudaEventSynchronize(r->ev1));
+  CUDA_TRY(cudaEventElapsedTime(ms, r->ev0, r->ev1));
+  return PYR3_OK;
+}
+
+// ---------------------------------------------------------------- present
+static int run_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t total_samples,
+                       void* dev_out, int32_t out_kind) {
+  if (out_kind != PYR3_OUT_RGBA8 && out_kind != PYR3_OUT_RGBA32F)
+    return fail(PYR3_E_INVALID, "unknown output kind");
+  if (total_samples == 0) return fail(PYR3_E_INVALID, "total_samples must be positive");
+  // src/calibration.ts:37-43 in double, uploaded as f32.
+  const double os2 = (double)r->os * (double)r->os;
+  const float k1 = (float)((p->brightness * 255.0 * 268.0) / 256.0);
+  const float k2 = (float)((os2 * p->scale * p->scale) / (255.0 * (double)total_samples));
+  const float* filtered = nullptr;
+  if (p->density_on) {
+    int rc = ensure_filtered(r);
+    if (rc) return rc;
+    pyr3::DeParams d;
+    d.width = r->SW;
+    d.height = r->SH;
+    d.max_rad = (float)((double)p->de_max_rad * r->os + 1.0);
+    d.min_rad = (float)((double)p->de_min_rad * r->os + 1.0);
+    d.curve = p->de_curve;
+    d.k1 = k1;
+    d.k2 = k2;
+    d.R = (int)std::ceil(std::min(std::max(d.max_rad, 0.0f), 256.0f));
+    CUDA_TRY(pyr3::launch_density(r->d_hist, r->d_filtered, d, r->d_knorm, r->d_kwtab, r->stream));
+    filtered = r->d_filtered;
+  }
+  pyr3::TonemapParams t;
+  t.width = r->W;
+  t.height = r->H;
+  t.oversample = r->os;
+  t.fwidth = (uint32_t)r->fwidth;
+  t.k1 = k1;
+  t.k2 = k2;
+  t.gamma = p->gamma;
+  t.vibrancy = p->vibrancy;
+  t.highpow = p->highpow;
+  t.linrange = p->linrange;
+  t.bg[0] = p->background[0];
+  t.bg[1] = p->background[1];
+  t.bg[2] = p->background[2];
+  t.transparent = p->transparent;
+  CUDA_TRY(pyr3::launch_tonemap(filtered ? nullptr : r->d_hist, filtered, t, r->d_kern, dev_out,
+                                out_kind == PYR3_OUT_RGBA8, r->stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_present_device(pyr3_renderer* r, const pyr3_present_opts* p,
+                                 uint64_t total_samples, void* device_out, int32_t out_kind) {
+  if (!r || !p || !device_out) return fail(PYR3_E_INVALID, "null argument");
+  cudaSetDevice(r->device);
+  return run_present(r, p, total_samples, device_out, out_kind);
+}
+
+PYR3_API int pyr3_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t total_samples,
+                          void* out, int32_t out_kind) {
+  if (!r || !p || !out) return fail(PYR3_E_INVALID, "null argument");
+  cudaSetDevice(r->device);
+  const size_t bytes = (size_t)r->W * r->H * (out_kind == PYR3_OUT_RGBA8 ? 4 : 16);
+  int rc = ensure_out(r, bytes);
+  if (rc) return rc;
+  rc = run_present(r, p, total_samples, r->d_out, out_kind);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(out, r->d_out, bytes, cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_read_histogram(pyr3_renderer* r, uint32_t* host_out) {
+  if (!r || !host_out) return fail(PYR3_E_INVALID, "null argument");
+  cudaSetDevice(r->device);
+  CUDA_TRY(cudaMemcpyAsync(host_out, r->d_hist, (size_t)r->SW * r->SH * 16, cudaMemcpyDeviceToHost,
+                           r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_read_index_map(pyr3_renderer* r, uint32_t* host_out) {
+  if (!r || !host_out) return fail(PYR3_E_INVALID, "null argument");
+  cudaSetDevice(r->device);
+  CUDA_TRY(cudaMemcpyAsync(host_out, r->d_idx, (size_t)r->SW * r->SH * 4, cudaMemcpyDeviceToHost,
+                           r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_sync(pyr3_renderer* r) {
+  if (!r) return fail(PYR3_E_INVALID, "null renderer");
+  cudaSetDevice(r->device);
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_info(pyr3_renderer* r, uint32_t* super_w, uint32_t* super_h, void** device_hist) {
+  if (!r) return fail(PYR3_E_INVALID, "null renderer");
+  if (super_w) *super_w = r->SW;
+  if (super_h) *super_h = r->SH;
+  if (device_hist) *device_hist = r->d_hist;
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_counters(pyr3_renderer* r, uint64_t* samples, uint64_t* splats) {
+  if (!r) return fail(PYR3_E_INVALID, "null renderer");
+  uint64_t c[2] = {0, 0};
+  cudaSetDevice(r->device);
+  CUDA_TRY(cudaMemcpyAsync(c, r->d_counters, 16, cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  if (samples) *samples = c[0];
+  if (splats) *splats = c[1];
+  return PYR3_OK;
+}
+
+// ------------------------------------------------------ stage entry points
+namespace {
+// A throw-away genome shape of n linear xforms, for the pick / splat /
+// seed stage kernels that live in the chaos module.
+int stage_module(int n, std::shared_ptr<pyr3::ChaosModule>* m) {
+  std::vector<float> xf((size_t)n * 116, 0.0f);
+  for (int k = 0; k < n; ++k) {
+    xf[(size_t)k * 116 + 7] = 1.0f;   // one variation
+    xf[(size_t)k * 116 + 21] = 1.0f;  // linear, weight 1
+  }
+  pyr3::GenomeShape s;
+  std::string e = pyr3::shape_from_packed(xf.data(), n, -1, &s);
+  if (!e.empty()) return fail(PYR3_E_INVALID, e);
+  std::string err;
+  int rc = pyr3::get_chaos_module(s, kWpb, false, m, &err);
+  if (rc) return fail(rc, err);
+  return PYR3_OK;
+}
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  ~DevBuf() { cudaFree(p); }
+};
+}  // namespace
+
+PYR3_API int pyr3_seed_walkers(uint32_t seed, uint64_t base, uint32_t n, uint32_t* host_out) {
+  if (!host_out || n == 0) return fail(PYR3_E_INVALID, "bad arguments");
+  int rc = set_device(0);
+  if (rc) return rc;
+  std::shared_ptr<pyr3::ChaosModule> m;
+  rc = stage_module(1, &m);
+  if (rc) return rc;
+  DevBuf<uint32_t> d;
+  CUDA_TRY(cudaMalloc(&d.p, (size_t)n * 36 * 4));
+  void* params[] = {&seed, &base, &n, &d.p};
+  LAUNCH_TRY(m->seed_test, (n + kWpb - 1) / kWpb, kWpb, 0, nullptr, params);
+  CUDA_TRY(cudaMemcpy(host_out, d.p, (size_t)n * 36 * 4, cudaMemcpyDeviceToHost));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_eval_variation(uint32_t idx, uint32_t n, const float* pts_xy, float weight,
+                                 const float* params10, const float* a0, const float* a1,
+                                 uint32_t* isaac, float* out_xy) {
+  if (!pts_xy || !params10 || !a0 || !a1 || !isaac || !out_xy || n == 0)
+    return fail(PYR3_E_INVALID, "bad arguments");
+  int rc = set_device(0);
+  if (rc) return rc;
+  std::shared_ptr<pyr3::EvalModule> m;
+  std::string err;
+  rc = pyr3::get_eval_module((int)idx, &m, &err);
+  if (rc) return fail(rc, err);
+  DevBuf<float> dp, dprm, dout;
+  DevBuf<uint32_t> dst;
+  CUDA_TRY(cudaMalloc(&dp.p, (size_t)n * 8));
+  CUDA_TRY(cudaMalloc(&dout.p, (size_t)n * 8));
+  CUDA_TRY(cudaMalloc(&dprm.p, 40));
+  CUDA_TRY(cudaMalloc(&dst.p, (size_t)n * 144));
+  CUDA_TRY(cudaMemcpy(dp.p, pts_xy, (size_t)n * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dprm.p, params10, 40, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dst.p, isaac, (size_t)n * 144, cudaMemcpyHostToDevice));
+  float4 A0 = make_float4(a0[0], a0[1], a0[2], a0[3]), A1 = make_float4(a1[0], a1[1], a1[2], a1[3]);
+  void* params[] = {&n, &dp.p, &weight, &dprm.p, &A0, &A1, &dst.p, &dout.p};
+  LAUNCH_TRY(m->eval, (n + 127) / 128, 128, 0, nullptr, params);
+  CUDA_TRY(cudaMemcpy(out_xy, dout.p, (size_t)n * 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(isaac, dst.p, (size_t)n * 144, cudaMemcpyDeviceToHost));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_eval_dc_color(uint32_t idx, uint32_t n, const float* pts_xy, const float* v4,
+                                const float* ve4, float* out_rgb, int32_t* hit) {
+  if (!pts_xy || !v4 || !ve4 || !out_rgb || !hit || n == 0) return fail(PYR3_E_INVALID, "bad arguments");
+  if (!pyr3::variation_is_dc((int)idx)) {
+    for (uint32_t i = 0; i < n; ++i) hit[i] = 0;
+    std::memset(out_rgb, 0, (size_t)n * 12);
+    return PYR3_OK;
+  }
+  int rc = set_device(0);
+  if (rc) return rc;
+  std::shared_ptr<pyr3::EvalModule> m;
+  std::string err;
+  rc = pyr3::get_eval_module((int)idx, &m, &err);
+  if (rc) return fail(rc, err);
+  if (!m->dc) return fail(PYR3_E_UNSUPPORTED, "no direct colour kernel");
+  const float prm[10] = {v4[2], v4[3], ve4[0], ve4[1], ve4[2], ve4[3], 0, 0, 0, 0};
+  DevBuf<float> dp, dprm, dout;
+  CUDA_TRY(cudaMalloc(&dp.p, (size_t)n * 8));
+  CUDA_TRY(cudaMalloc(&dout.p, (size_t)n * 12));
+  CUDA_TRY(cudaMalloc(&dprm.p, 40));
+  CUDA_TRY(cudaMemcpy(dp.p, pts_xy, (size_t)n * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dprm.p, prm, 40, cudaMemcpyHostToDevice));
+  void* params[] = {&n, &dp.p, &dprm.p, &dout.p};
+  LAUNCH_TRY(m->dc, (n + 127) / 128, 128, 0, nullptr, params);
+  CUDA_TRY(cudaMemcpy(out_rgb, dout.p, (size_t)n * 12, cudaMemcpyDeviceToHost));
+  for (uint32_t i = 0; i < n; ++i) hit[i] = 1;
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_pick_stream(uint32_t n_xforms, const float* weights, const float* xaos,
+                              uint32_t count, const int32_t* prev, const uint32_t* draws,
+                              uint32_t* out) {
+  if (!weights || !prev || !draws || !out || n_xforms == 0 || n_xforms > PYR3_MAX_XFORMS || count == 0)
+    return fail(PYR3_E_INVALID, "bad arguments");
+  int rc = set_device(0);
+  if (rc) return rc;
+  std::vector<uint16_t> starts;
+  std::string err;
+  if (!build_pick_starts((int)n_xforms, weights, xaos, &starts, &err)) return fail(PYR3_E_INVALID, err);
+  std::shared_ptr<pyr3::ChaosModule> m;
+  rc = stage_module((int)n_xforms, &m);
+  if (rc) return rc;
+  DevBuf<uint16_t> dst;
+  DevBuf<int32_t> dprev;
+  DevBuf<uint32_t> ddraw, dout;
+  CUDA_TRY(cudaMalloc(&dst.p, starts.size() * 2));
+  CUDA_TRY(cudaMalloc(&dprev.p, (size_t)count * 4));
+  CUDA_TRY(cudaMalloc(&ddraw.p, (size_t)count * 4));
+  CUDA_TRY(cudaMalloc(&dout.p, (size_t)count * 4));
+  CUDA_TRY(cudaMemcpy(dst.p, starts.data(), starts.size() * 2, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dprev.p, prev, (size_t)count * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(ddraw.p, draws, (size_t)count * 4, cudaMemcpyHostToDevice));
+  void* params[] = {&dst.p, &count, &dprev.p, &ddraw.p, &dout.p};
+  LAUNCH_TRY(m->pick_test, (count + 255) / 256, 256, 0, nullptr, params);
+  CUDA_TRY(cudaMemcpy(out, dout.p, (size_t)count * 4, cudaMemcpyDeviceToHost));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_splat_points(uint32_t n, const float* pts, uint32_t width, uint32_t height,
+                               float scale, float cx, float cy, float rotation_rad,
+                               uint32_t palette_mode, const float* palette, int32_t aggregate,
+                               uint32_t* hist_inout) {
+  if (!pts || !palette || !hist_inout || n == 0 || width == 0 || height == 0)
+    return fail(PYR3_E_INVALID, "bad arguments");
+  int rc = set_device(0);
+  if (rc) return rc;
+  std::shared_ptr<pyr3::ChaosModule> m;
+  {
+    std::vector<float> xf(116, 0.0f);
+    xf[7] = 1.0f;
+    xf[21] = 1.0f;
+    pyr3::GenomeShape s;
+    pyr3::shape_from_packed(xf.data(), 1, -1, &s);
+    std::string err;
+    rc = pyr3::get_chaos_module(s, kWpb, aggregate != 0, &m, &err);
+    if (rc) return fail(rc, err);
+  }
+  const size_t hb = (size_t)width * height * 16;
+  DevBuf<float> dpts, dpal;
+  DevBuf<uint32_t> dh;
+  DevBuf<uint64_t> dcnt;
+  CUDA_TRY(cudaMalloc(&dpts.p, (size_t)n * 16));
+  CUDA_TRY(cudaMalloc(&dpal.p, 4096));
+  CUDA_TRY(cudaMalloc(&dh.p, hb));
+  CUDA_TRY(cudaMalloc(&dcnt.p, 16));
+  CUDA_TRY(cudaMemcpy(dpts.p, pts, (size_t)n * 16, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dpal.p, palette, 4096, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dh.p, hist_inout, hb, cudaMemcpyHostToDevice));
+  ChaosArgs A;
+  std::memset(&A, 0, sizeof A);
+  A.hist = dh.p;
+  A.palette = dpal.p;
+  A.width = width;
+  A.height = height;
+  A.scale = scale;
+  A.cx = cx;
+  A.cy = cy;
+  A.cos_r = std::cos(rotation_rad);
+  A.sin_r = std::sin(rotation_rad);
+  A.palette_mode = palette_mode;
+  A.counters = dcnt.p;
+  void* params[] = {&A, &n, &dpts.p};
+  LAUNCH_TRY(m->splat_test, (n + kWpb - 1) / kWpb, kWpb, 0, nullptr, params);
+  CUDA_TRY(cudaMemcpy(hist_inout, dh.p, hb, cudaMemcpyDeviceToHost));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_density_tonemap(const uint32_t* hist, uint32_t width, uint32_t height,
+                                  uint32_t oversample, float filter_radius,
+                                  const pyr3_present_opts* p, uint64_t total_samples,
+                                  float* out_rgba, float* filtered_out) {
+  if (!hist || !p || !out_rgba || oversample == 0 || width == 0 || height == 0)
+    return fail(PYR3_E_INVALID, "bad arguments");
+  pyr3_opts o{width, height, oversample, filter_radius, 0};
+  pyr3_renderer* r = nullptr;
+  int rc = pyr3_create(&o, &r);
+  if (rc) return rc;
+  std::unique_ptr<pyr3_renderer, int (*)(pyr3_renderer*)> guard(r, pyr3_destroy);
+  CUDA_TRY(cudaMemcpyAsync(r->d_hist, hist, (size_t)r->SW * r->SH * 16, cudaMemcpyHostToDevice, r->stream));
+  rc = pyr3_present(r, p, total_samples, out_rgba, PYR3_OUT_RGBA32F);
+  if (rc) return rc;
+  if (filtered_out && p->density_on)
+    CUDA_TRY(cudaMemcpy(filtered_out, r->d_filtered, (size_t)r->SW * r->SH * 16, cudaMemcpyDeviceToHost));
+  return PYR3_OK;
+}
+
+// ------------------------------------------------------------ build checks
+PYR3_API int pyr3_jit_compile(const pyr3_genome* g, int32_t aggregate, uint64_t* cubin_bytes) {
+  if (!g || !g->xforms) return fail(PYR3_E_INVALID, "null genome");
+  pyr3::GenomeShape shape;
+  std::string e = pyr3::shape_from_packed(g->xforms, (int)g->n_xforms, g->final_slot, &shape);
+  if (!e.empty())
+    return fail(e.find("not implemented") != std::string::npos ? PYR3_E_UNSUPPORTED : PYR3_E_INVALID, e);
+  size_t n = 0;
+  std::string err;
+  int rc = pyr3::compile_chaos_only(shape, kWpb, aggregate != 0, &n, &err);
+  if (rc) return fail(rc, err);
+  if (cubin_bytes) *cubin_bytes = n;
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_jit_source(const pyr3_genome* g, char* buf, uint64_t cap, uint64_t* len) {
+  if (!g || !g->xforms) return fail(PYR3_E_INVALID, "null genome");
+  pyr3::GenomeShape shape;
+  std::string e = pyr3::shape_from_packed(g->xforms, (int)g->n_xforms, g->final_slot, &shape);
+  if (!e.empty()) return fail(PYR3_E_INVALID, e);
+  std::string src = pyr3::chaos_source(shape, kWpb, false);
+  if (len) *len = src.size();
+  if (buf && cap) {
+    size_t n = std::min<size_t>(cap - 1, src.size());
+    std::memcpy(buf, src.data(), n);
+    buf[n] = 0;
+  }
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_jit_compile_variation(uint32_t idx, uint64_t* cubin_bytes) {
+  size_t n = 0;
+  std::string err;
+  int rc = pyr3::compile_eval_only((int)idx, &n, &err);
+  if (rc) return fail(rc, err);
+  if (cubin_bytes) *cubin_bytes = n;
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_variation_info(uint32_t idx, int32_t* implemented, int32_t* is_dc,
+                                 const char** name) {
+  if (idx >= (uint32_t)pyr3::kNumVariations) return fail(PYR3_E_INVALID, "index out of range");
+  if (implemented) *implemented = pyr3::variation_implemented((int)idx) ? 1 : 0;
+  if (is_dc) *is_dc = pyr3::variation_is_dc((int)idx) ? 1 : 0;
+  if (name) *name = pyr3::variation_name((int)idx);
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_pick_table(uint32_t n_xforms, const float* weights, const float* xaos,
+                             uint32_t* table_out) {
+  if (!weights || !table_out || n_xforms == 0 || n_xforms > PYR3_MAX_XFORMS)
+    return fail(PYR3_E_INVALID, "bad arguments");
+  std::vector<uint16_t> starts;
+  std::string err;
+  const int n = (int)n_xforms;
+  if (!build_pick_starts(n, weights, xaos, &starts, &err)) return fail(PYR3_E_INVALID, err);
+  for (int r = 0; r <= n; ++r) {
+    const uint16_t* st = starts.data() + (size_t)r * n;
+    for (uint32_t g = 0; g < kGrain; ++g) {
+      uint32_t v = 0;
+      for (int j = 1; j < n; ++j) v += g >= st[j] ? 1u : 0u;
+      table_out[(size_t)r * kGrain + g] = v;
+    }
+  }
+  return PYR3_OK;
+}
+
+// ------------------------------------------------------------------ timing
+PYR3_API int pyr3_mark(pyr3_renderer* r, int32_t slot) {
+  if (!r || slot < 0 || slot >= 8) return fail(PYR3_E_INVALID, "bad timing slot");
+  cudaSetDevice(r->device);
+  if (!r->marks[slot]) CUDA_TRY(cudaEventCreate(&r->marks[slot]));
+  CUDA_TRY(cudaEventRecord(r->marks[slot], r->stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_elapsed(pyr3_renderer* r, int32_t a, int32_t b, float* ms) {
+  if (!r || !ms || a < 0 || a >= 8 || b < 0 || b >= 8 || !r->marks[a] || !r->marks[b])
+    return fail(PYR3_E_INVALID, "bad timing slots");
+  cudaSetDevice(r->device);
+  CUDA_TRY(cudaEventSynchronize(r->marks[b]));
+  CUDA_TRY(cudaEventElapsedTime(ms, r->marks[a], r->marks[b]));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_flush_l2(pyr3_renderer* r, uint64_t bytes) {
+  if (!r) return fail(PYR3_E_INVALID, "null renderer");
+  cudaSetDevice(r->device);
+  if (r->flush_bytes < bytes) {
+    CUDA_TRY(cudaStreamSynchronize(r->stream));
+    cudaFree(r->d_flush);
+    r->d_flush = nullptr;
+    CUDA_TRY(cudaMalloc(&r->d_flush, bytes));
+    r->flush_bytes = bytes;
+  }
+  CUDA_TRY(cudaMemsetAsync(r->d_flush, 0x5a, bytes, r->stream));
+  return PYR3_OK;
+}

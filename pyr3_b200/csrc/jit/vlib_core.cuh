@@ -1,0 +1,233 @@
+// pyr3-b200 variation library: core helpers shared by every variation.
+//
+// Compiled at run time by NVRTC (sm_100a) together with the generated chaos
+// kernel for one genome structure.  No CUDA headers are included: NVRTC
+// provides the math builtins.
+//
+// Numeric contract (the reference's WGSL semantics, chaos.wgsl:230-520):
+//   * all iteration arithmetic is f32;
+//   * trig of |a| > 1e6 is replaced by trig of a hash of the argument bits
+//     (safe_sin/safe_cos, chaos.wgsl:356-372), tanh clamps its argument to
+//     +-20 (chaos.wgsl:381-385);
+//   * pow(x < 0, y) is NaN (GPU exp2(y*log2 x) semantics), float x % y is
+//     x - y*trunc(x/y), round() is round-half-even, f32->int conversions
+//     clamp (WGSL value conversion);
+//   * RNG: one ISAAC (RANDSIZL=4) stream per walker, rand01 / rand_11 scale
+//     the low 28 bits exactly as chaos.wgsl:319-331 / flam3.c:2625-2631.
+#pragma once
+
+typedef unsigned int u32;
+typedef int i32;
+typedef unsigned long long u64;
+
+#define VDEV __device__ __forceinline__
+
+#define P_PI 3.14159265358979323846f
+#define P_TAU 6.28318530717958647692f
+#define P_HALF_PI 1.57079632679489661923f
+#define P_EPS 1e-10f
+#define P_LN10 2.302585092994046f
+
+// ----------------------------------------------------------------- float2
+VDEV float2 f2(float x, float y) { return make_float2(x, y); }
+VDEV float2 operator+(float2 a, float2 b) { return f2(a.x + b.x, a.y + b.y); }
+VDEV float2 operator-(float2 a, float2 b) { return f2(a.x - b.x, a.y - b.y); }
+VDEV float2 operator-(float2 a) { return f2(-a.x, -a.y); }
+VDEV float2 operator*(float2 a, float s) { return f2(a.x * s, a.y * s); }
+VDEV float2 operator*(float s, float2 a) { return f2(s * a.x, s * a.y); }
+VDEV float2 operator*(float2 a, float2 b) { return f2(a.x * b.x, a.y * b.y); }
+VDEV float2 operator/(float2 a, float s) { return f2(a.x / s, a.y / s); }
+VDEV float2& operator+=(float2& a, float2 b) { a.x += b.x; a.y += b.y; return a; }
+VDEV float dot2(float2 a, float2 b) { return a.x * b.x + a.y * b.y; }
+VDEV float sq2(float2 a) { return a.x * a.x + a.y * a.y; }
+VDEV float len2(float2 a) { return sqrtf(a.x * a.x + a.y * a.y); }
+
+// ------------------------------------------------------- WGSL semantics
+VDEV float wpow(float x, float y) {
+  return x < 0.0f ? __int_as_float(0x7fffffff) : powf(x, y);
+}
+VDEV float wmod(float x, float y) { return x - y * truncf(x / y); }
+VDEV float wfract(float x) { return x - floorf(x); }
+VDEV float wround(float x) { return rintf(x); }
+VDEV float wsign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+VDEV float wclamp(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+VDEV float wmix(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+VDEV float wstep(float edge, float x) { return edge <= x ? 1.0f : 0.0f; }
+VDEV float wsmooth(float lo, float hi, float x) {
+  float t = wclamp((x - lo) / (hi - lo), 0.0f, 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+VDEV i32 f2i(float v) {  // WGSL i32(f32): truncate, clamp, NaN -> 0
+  if (!(v == v)) return 0;
+  return v <= -2147483648.0f ? (i32)0x80000000 : (v >= 2147483520.0f ? 2147483520 : (i32)v);
+}
+VDEV u32 f2u(float v) {  // WGSL u32(f32)
+  if (!(v > 0.0f)) return 0u;
+  return v >= 4294967040.0f ? 4294967040u : (u32)v;
+}
+VDEV i32 imod(i32 a, i32 b) {  // WGSL i32 %: x % 0 = 0
+  return b == 0 ? 0 : ((a == (i32)0x80000000 && b == -1) ? 0 : a % b);
+}
+VDEV i32 idiv(i32 a, i32 b) {  // WGSL i32 /: x / 0 = x
+  return b == 0 ? a : ((a == (i32)0x80000000 && b == -1) ? a : a / b);
+}
+
+// ------------------------------------------------------------ safe trig
+VDEV float hash01(u32 h) {
+  h ^= h >> 17; h *= 0xed5ad4bbu;
+  h ^= h >> 11; h *= 0xac4c1b51u;
+  h ^= h >> 15;
+  return (float)h * (1.0f / 4294967296.0f);
+}
+VDEV float ssin(float a) {
+  return fabsf(a) <= 1.0e6f ? sinf(a) : sinf(hash01(__float_as_uint(a)) * P_TAU);
+}
+VDEV float scos(float a) {
+  return fabsf(a) <= 1.0e6f ? cosf(a) : cosf(hash01(__float_as_uint(a)) * P_TAU);
+}
+VDEV void ssincos(float a, float* s, float* c) {
+  float t = fabsf(a) <= 1.0e6f ? a : hash01(__float_as_uint(a)) * P_TAU;
+  sincosf(t, s, c);
+}
+VDEV float stan(float a) { return ssin(a) / scos(a); }
+VDEV float stanh(float a) { return tanhf(wclamp(a, -20.0f, 20.0f)); }
+VDEV float2 polar2(float r, float ang) {  // (r cos a, r sin a) with safe trig
+  float s, c;
+  ssincos(ang, &s, &c);
+  return f2(r * c, r * s);
+}
+
+// ------------------------------------------------------------ RNG state
+// One ISAAC stream per walker, held in shared memory as a [36][W] array of
+// u32 so that a warp touching 32 consecutive walkers hits 32 banks whatever
+// field it reads: field 0 = cnt, 1..3 = a, b, c, 4..19 = mem, 20..35 = rsl.
+struct Rng {
+  u32* s;  // &state[0][walker]
+  u32 W;   // walkers per block (stride between fields)
+  VDEV u32& f(u32 k) const { return s[k * W]; }
+};
+
+// One ISAAC round (Jenkins' isaac() with RANDSIZL = 4), flam3 isaac.c.
+VDEV void isaac_round(const Rng& r) {
+  u32 a = r.f(1);
+  u32 c = r.f(3) + 1u;
+  r.f(3) = c;
+  u32 b = r.f(2) + c;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int m = i, m2 = (i + 8) & 15;
+    u32 mixed;
+    switch (i & 3) {
+      case 0: mixed = a ^ (a << 13); break;
+      case 1: mixed = a ^ (a >> 6); break;
+      case 2: mixed = a ^ (a << 2); break;
+      default: mixed = a ^ (a >> 16); break;
+    }
+    u32 x = r.f(4 + m);
+    a = mixed + r.f(4 + m2);
+    u32 y = r.f(4 + ((x >> 2) & 15u)) + a + b;
+    r.f(4 + m) = y;
+    b = r.f(4 + ((y >> 6) & 15u)) + x;
+    r.f(20 + m) = b;
+  }
+  r.f(1) = a;
+  r.f(2) = b;
+}
+
+VDEV u32 irand(const Rng& r) {
+  u32 cnt = r.f(0);
+  if (cnt == 0u) {
+    isaac_round(r);
+    cnt = 15u;
+  } else {
+    cnt -= 1u;
+  }
+  r.f(0) = cnt;
+  return r.f(20 + cnt);
+}
+VDEV float rand01(const Rng& r) {
+  return (float)(irand(r) & 0x0fffffffu) * (1.0f / 268435455.0f);
+}
+VDEV float rand_11(const Rng& r) {
+  return (float)((i32)(irand(r) & 0x0fffffffu) - 0x07ffffff) * (1.0f / 134217727.0f);
+}
+
+// ------------------------------------------------------ variation context
+// Everything a variation may read besides its input point, weight and its
+// ten parameters: the walker's RNG and the owning xform's affine
+// coefficients (a0 = [a, b, c, weight], a1 = [d, e, f, nvars]).
+struct Ctx {
+  Rng rng;
+  float4 a0, a1;
+};
+
+#define VAR(name) VDEV float2 var_##name(float2 p, float w, const float* __restrict__ P, Ctx& c)
+#define RAND01() rand01(c.rng)
+#define RAND11() rand_11(c.rng)
+#define IRAND() irand(c.rng)
+
+// --------------------------------------------------------------- complex
+// z = (re, im).  Division / reciprocal floor |b|^2 at 0 (the reference's
+// 1e-100 floor rounds to 0 in f32).
+VDEV float2 cmul(float2 a, float2 b) { return f2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+VDEV float2 csqr(float2 z) { return f2(z.x * z.x - z.y * z.y, 2.0f * z.x * z.y); }
+VDEV float2 cdiv(float2 a, float2 b) {
+  float m2 = fmaxf(dot2(b, b), 0.0f);
+  return f2((a.x * b.x + a.y * b.y) / m2, (a.y * b.x - a.x * b.y) / m2);
+}
+VDEV float2 crecip(float2 z) {
+  float m2 = fmaxf(dot2(z, z), 0.0f);
+  return f2(z.x / m2, -z.y / m2);
+}
+VDEV float2 csqrt(float2 z) {
+  float rad = len2(z);
+  float sb = z.y < 0.0f ? -1.0f : 1.0f;
+  return f2(sqrtf(fmaxf(0.5f * (rad + z.x), 0.0f)), sb * sqrtf(fmaxf(0.5f * (rad - z.x), 0.0f)));
+}
+VDEV float2 clog(float2 z) {
+  return f2(0.5f * logf(dot2(z, z) + 1e-20f), atan2f(z.y, z.x));
+}
+VDEV float2 cexp(float2 z) {
+  float e = expf(wclamp(z.x, -20.0f, 20.0f));
+  float s, co;
+  ssincos(z.y, &s, &co);
+  return f2(e * co, e * s);
+}
+VDEV float2 cpowc(float2 t, float2 p) { return cexp(cmul(p, clog(t))); }
+VDEV float2 csin(float2 z) {
+  float y = wclamp(z.y, -20.0f, 20.0f);
+  float ep = expf(y), en = expf(-y);
+  float ch = 0.5f * (ep + en), sh = 0.5f * (ep - en);
+  return f2(ssin(z.x) * ch, scos(z.x) * sh);
+}
+
+// ----------------------------------------------------------------- colour
+// hsv_to_rgb (chaos.wgsl:1662): v * mix(1, clamp(|fract(h + k)*6 - 3| - 1),
+// s) with k = (1, 2/3, 1/3).
+VDEV float3 hsv_rgb(float h, float s, float v) {
+  const float k[3] = {1.0f, 2.0f / 3.0f, 1.0f / 3.0f};
+  float o[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float q = fabsf(wfract(h + k[i]) * 6.0f - 3.0f);
+    o[i] = v * wmix(1.0f, wclamp(q - 1.0f, 0.0f, 1.0f), s);
+  }
+  return make_float3(o[0], o[1], o[2]);
+}
+// hsl_to_rgb (chaos.wgsl:1696).
+VDEV float3 hsl_rgb(float hh, float ss, float ll) {
+  float h = wfract(hh), s = wclamp(ss, 0.0f, 1.0f), l = wclamp(ll, 0.0f, 1.0f);
+  float cc = (1.0f - fabsf(2.0f * l - 1.0f)) * s;
+  float h6 = h * 6.0f;
+  float x = cc * (1.0f - fabsf((h6 - 2.0f * floorf(h6 * 0.5f)) - 1.0f));
+  float m = l - cc * 0.5f;
+  float r, g, b;
+  if (h6 < 1.0f) { r = cc; g = x; b = 0.0f; }
+  else if (h6 < 2.0f) { r = x; g = cc; b = 0.0f; }
+  else if (h6 < 3.0f) { r = 0.0f; g = cc; b = x; }
+  else if (h6 < 4.0f) { r = 0.0f; g = x; b = cc; }
+  else if (h6 < 5.0f) { r = x; g = 0.0f; b = cc; }
+  else { r = cc; g = 0.0f; b = x; }
+  return make_float3(r + m, g + m, b + m);
+}
+#define DCV(name) VDEV float3 dc_##name(float2 p, const float* __restrict__ P)

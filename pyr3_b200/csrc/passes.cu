@@ -1,0 +1,309 @@
+// Density estimation and tonemap passes (nvcc, sm_100a).
+//
+// Density estimation restates density_main (src/shaders/density.wgsl:51-123)
+// in its scatter form: every non-empty bucket spreads
+//   w(d) = exp(-d^2 / (2 sigma^2)) / knorm[r] * ls,   sigma = r / 3,
+//   r = round(clamp(max_rad / (hits + 1)^curve, min_rad, max_rad)),
+//   ls = k1 * log(1 + count * k2) / count
+// over its own disc d^2 <= r^2.  The reference gathers (2R+1)^2 neighbours
+// per output pixel; the scatter form does work proportional to each
+// bucket's own disc, which is 10-1000x less on dense attractors.  Each CTA
+// owns a TILE x TILE output tile accumulated in shared memory (float
+// atomics); it streams the buckets of the tile plus an R halo with 128-bit
+// loads, and small discs are splatted by the thread that read them while
+// large discs are queued and splatted cooperatively by a whole warp.
+//
+// Tonemap restates the visualize fragment shader (src/shaders/
+// visualize_u32.wgsl:147-248 and visualize_f32.wgsl:162-271): fw x fw
+// spatial-filter collapse of the super-res source (per-tap log-density ls
+// for the raw histogram), flam3 alpha / vibrancy / highlight-power
+// composite, background blend, clamp; curves and HSL adjustments are off.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "passes.h"
+
+namespace pyr3 {
+
+// ------------------------------------------------------------- density
+constexpr int kTile = 32;
+constexpr int kDeThreads = 256;
+constexpr int kBigQueue = 512;    // large-disc queue entries per tile
+constexpr int kBigRadius = 3;     // discs with r > this go to the warp queue
+constexpr int kKwMaxR = 64;       // weight table covers r <= 64
+
+__device__ __forceinline__ int kw_offset(int r) {  // sum_{q<r} (q^2 + 1)
+  return (r * (r - 1) * (2 * r - 1)) / 6 + r;
+}
+
+// kw_table[offset(r) + d2] = exp(-d2 / (2 sigma^2)) / max(knorm[r], 1e-6),
+// exactly the reference's per-tap expression (density.wgsl:107-113).
+__global__ void k_kw_table(const float* __restrict__ knorm, float* __restrict__ tab) {
+  const int r = blockIdx.x;
+  const float rad = (float)r;
+  const float sig = fmaxf(rad / 3.0f, 1e-6f);
+  const float kn = fmaxf(knorm[r], 1e-6f);
+  for (int d2 = threadIdx.x; d2 <= r * r; d2 += blockDim.x) {
+    const float kw = expf(-(float)d2 / (2.0f * sig * sig));
+    tab[kw_offset(r) + d2] = kw / kn;
+  }
+}
+
+struct DeBucket {
+  int sx, sy, r;
+  float4 v;  // hist RGBA * ls
+};
+
+__device__ __forceinline__ void de_disc(const DeBucket& b, int tx0, int ty0, float4* acc,
+                                        const float* __restrict__ tab, const float* __restrict__ knorm,
+                                        int lane, int step) {
+  // footprint of the disc clipped to the tile
+  const int x0 = max(b.sx - b.r, tx0), x1 = min(b.sx + b.r, tx0 + kTile - 1);
+  const int y0 = max(b.sy - b.r, ty0), y1 = min(b.sy + b.r, ty0 + kTile - 1);
+  if (x0 > x1 || y0 > y1) return;
+  const int wdt = x1 - x0 + 1;
+  const int n = wdt * (y1 - y0 + 1);
+  const int r2 = b.r * b.r;
+  const float* row = b.r <= kKwMaxR ? tab + kw_offset(b.r) : nullptr;
+  const float rad = (float)b.r;
+  const float sig = fmaxf(rad / 3.0f, 1e-6f);
+  const float kn = b.r <= kKwMaxR ? 0.0f : fmaxf(knorm[min(b.r, 256)], 1e-6f);
+  for (int k = lane; k < n; k += step) {
+    const int x = x0 + k % wdt, y = y0 + k / wdt;
+    const int dx = x - b.sx, dy = y - b.sy;
+    const int d2 = dx * dx + dy * dy;
+    if (d2 > r2) continue;
+    const float w = row ? row[d2] : expf(-(float)d2 / (2.0f * sig * sig)) / kn;
+    float* a = (float*)&acc[(y - ty0) * kTile + (x - tx0)];
+    atomicAdd(a + 0, b.v.x * w);
+    atomicAdd(a + 1, b.v.y * w);
+    atomicAdd(a + 2, b.v.z * w);
+    atomicAdd(a + 3, b.v.w * w);
+  }
+}
+
+__global__ void __launch_bounds__(kDeThreads)
+k_density(const uint4* __restrict__ hist, float4* __restrict__ out, DeParams p,
+          const float* __restrict__ knorm, const float* __restrict__ tab) {
+  __shared__ float4 acc[kTile * kTile];
+  __shared__ DeBucket big[kBigQueue];
+  __shared__ int n_big;
+  const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
+  for (int i = threadIdx.x; i < kTile * kTile; i += kDeThreads) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (threadIdx.x == 0) n_big = 0;
+  __syncthreads();
+
+  const int R = p.R;
+  const int hx0 = max(tx0 - R, 0), hx1 = min(tx0 + kTile - 1 + R, (int)p.width - 1);
+  const int hy0 = max(ty0 - R, 0), hy1 = min(ty0 + kTile - 1 + R, (int)p.height - 1);
+  const int hw = hx1 - hx0 + 1;
+  const int nsrc = hw * (hy1 - hy0 + 1);
+  for (int s = threadIdx.x; s < nsrc; s += kDeThreads) {
+    const int sx = hx0 + s % hw, sy = hy0 + s / hw;
+    const uint4 h = hist[(size_t)sy * p.width + sx];
+    const float nc = (float)h.w;
+    if (nc <= 0.0f) continue;
+    const float hits = nc / 255.0f;
+    const float rf = fminf(fmaxf(p.max_rad / powf(hits + 1.0f, p.curve), p.min_rad), p.max_rad);
+    const int r = min(max((int)rintf(rf), 0), 256);
+    // disc misses the tile entirely
+    if (sx + r < tx0 || sx - r > tx0 + kTile - 1 || sy + r < ty0 || sy - r > ty0 + kTile - 1) continue;
+    const float ls = (p.k1 * logf(1.0f + nc * p.k2)) / nc;
+    DeBucket b{sx, sy, r, make_float4((float)h.x * ls, (float)h.y * ls, (float)h.z * ls, nc * ls)};
+    if (r > kBigRadius) {
+      const int q = atomicAdd(&n_big, 1);
+      if (q < kBigQueue) {
+        big[q] = b;
+        continue;
+      }
+    }
+    de_disc(b, tx0, ty0, acc, tab, knorm, 0, 1);
+  }
+  __syncthreads();
+  const int nb = min(n_big, kBigQueue);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int q = warp; q < nb; q += kDeThreads / 32) de_disc(big[q], tx0, ty0, acc, tab, knorm, lane, 32);
+  __syncthreads();
+  for (int i = threadIdx.x; i < kTile * kTile; i += kDeThreads) {
+    const int x = tx0 + (i % kTile), y = ty0 + (i / kTile);
+    if (x < (int)p.width && y < (int)p.height) out[(size_t)y * p.width + x] = acc[i];
+  }
+}
+
+// -------------------------------------------------------------- tonemap
+__device__ __forceinline__ void rgb2hsv(const float c[3], float o[3]) {
+  const float mx = fmaxf(fmaxf(c[0], c[1]), c[2]);
+  const float mn = fminf(fminf(c[0], c[1]), c[2]);
+  const float d = mx - mn;
+  float h = 0.0f;
+  if (d > 0.0f) {
+    if (mx == c[0]) h = (c[1] - c[2]) / d;
+    else if (mx == c[1]) h = 2.0f + (c[2] - c[0]) / d;
+    else h = 4.0f + (c[0] - c[1]) / d;
+    h *= 60.0f;
+    if (h < 0.0f) h += 360.0f;
+  }
+  o[0] = h;
+  o[1] = mx > 0.0f ? d / mx : 0.0f;
+  o[2] = mx;
+}
+
+__device__ __forceinline__ void hsv2rgb(const float c[3], float o[3]) {
+  const float h = c[0] / 60.0f, s = c[1], v = c[2];
+  const float i = floorf(h), f = h - i;
+  const float pp = v * (1.0f - s), q = v * (1.0f - s * f), t = v * (1.0f - s * (1.0f - f));
+  float fi = i;  // WGSL i32(i) % 6 with a clamping conversion
+  int ix = fi != fi ? 0 : (fi <= -2147483648.0f ? INT32_MIN : (fi >= 2147483520.0f ? 2147483520 : (int)fi));
+  ix = ix % 6;
+  switch (ix) {
+    case 0: o[0] = v; o[1] = t; o[2] = pp; break;
+    case 1: o[0] = q; o[1] = v; o[2] = pp; break;
+    case 2: o[0] = pp; o[1] = v; o[2] = t; break;
+    case 3: o[0] = pp; o[1] = q; o[2] = v; break;
+    case 4: o[0] = t; o[1] = pp; o[2] = v; break;
+    default: o[0] = v; o[1] = pp; o[2] = q; break;
+  }
+}
+
+__device__ __forceinline__ float calc_alpha(float density, float g_inv, float linrange) {
+  if (density <= 0.0f) return 0.0f;
+  if (density < linrange) {
+    const float funcval = powf(linrange, g_inv);
+    const float frac = density / linrange;
+    return (1.0f - frac) * density * (funcval / linrange) + frac * powf(density, g_inv);
+  }
+  return powf(density, g_inv);
+}
+
+__device__ __forceinline__ void calc_newrgb(const float c[3], float ls, float highpow, float o[3]) {
+  if (ls == 0.0f || (c[0] == 0.0f && c[1] == 0.0f && c[2] == 0.0f)) {
+    o[0] = o[1] = o[2] = 0.0f;
+    return;
+  }
+  float sc[3];
+  for (int i = 0; i < 3; ++i) sc[i] = ls * (c[i] / 255.0f);
+  float maxa = sc[0], maxc = c[0] / 255.0f;
+  if (sc[1] > maxa) { maxa = sc[1]; maxc = c[1] / 255.0f; }
+  if (sc[2] > maxa) { maxa = sc[2]; maxc = c[2] / 255.0f; }
+  if (maxa > 255.0f && highpow >= 0.0f) {
+    const float newls = 255.0f / maxc;
+    const float lsratio = powf(newls / ls, highpow);
+    float nrgb[3], hsv[3];
+    for (int i = 0; i < 3; ++i) nrgb[i] = newls * (c[i] / 255.0f) / 255.0f;
+    rgb2hsv(nrgb, hsv);
+    hsv[1] *= lsratio;
+    hsv2rgb(hsv, nrgb);
+    for (int i = 0; i < 3; ++i) o[i] = nrgb[i] * 255.0f;
+  } else {
+    const float newls = 255.0f / maxc;
+    float adjhlp = -highpow;
+    if (adjhlp > 1.0f) adjhlp = 1.0f;
+    if (maxa <= 255.0f) adjhlp = 1.0f;
+    const float k = (1.0f - adjhlp) * newls + adjhlp * ls;
+    for (int i = 0; i < 3; ++i) o[i] = k * (c[i] / 255.0f);
+  }
+}
+
+template <bool kU32, bool kRgba8>
+__global__ void __launch_bounds__(256)
+k_tonemap(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapParams p,
+          const float* __restrict__ kern, void* __restrict__ out) {
+  __shared__ float kk[kMaxTaps];
+  if (threadIdx.x < p.fwidth) kk[threadIdx.x] = kern[threadIdx.x];
+  __syncthreads();
+  const uint32_t xi = blockIdx.x * 16 + (threadIdx.x & 15);
+  const uint32_t yi = blockIdx.y * 16 + (threadIdx.x >> 4);
+  if (xi >= p.width || yi >= p.height) return;
+  const int N = (int)p.oversample, fw = (int)p.fwidth, half = fw / 2;
+  const int sw = (int)p.width * N, sh = (int)p.height * N;
+  const int cx = (int)xi * N + N / 2, cy = (int)yi * N + N / 2;
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+  for (int dy = 0; dy < fw; ++dy) {
+    const float ky = kk[dy];
+    const int sy = min(max(cy + dy - half, 0), sh - 1);
+    for (int dx = 0; dx < fw; ++dx) {
+      const float kx = kk[dx];
+      const int sx = min(max(cx + dx - half, 0), sw - 1);
+      const size_t sb = (size_t)sy * sw + sx;
+      const float w = kx * ky;
+      if (kU32) {
+        const uint4 h = hu[sb];
+        const float cnt = (float)h.w;
+        if (cnt > 0.0f) {
+          const float ls = (p.k1 * logf(1.0f + cnt * p.k2)) / cnt;
+          s0 = s0 + ((float)h.x * ls) * w;
+          s1 = s1 + ((float)h.y * ls) * w;
+          s2 = s2 + ((float)h.z * ls) * w;
+          s3 = s3 + (cnt * ls) * w;
+        }
+      } else {
+        const float4 h = hf[sb];
+        s0 = s0 + h.x * w;
+        s1 = s1 + h.y * w;
+        s2 = s2 + h.z * w;
+        s3 = s3 + h.w * w;
+      }
+    }
+  }
+  float o[4];
+  if (s3 <= 0.0f) {
+    if (p.transparent) { o[0] = o[1] = o[2] = o[3] = 0.0f; }
+    else { o[0] = p.bg[0]; o[1] = p.bg[1]; o[2] = p.bg[2]; o[3] = 1.0f; }
+  } else {
+    const float g_inv = 1.0f / p.gamma;
+    const float tmp = s3 / 255.0f;
+    float alpha = calc_alpha(tmp, g_inv, p.linrange);
+    const float ls_a = p.vibrancy * 256.0f * alpha / fmaxf(tmp, 1e-12f);
+    alpha = fminf(fmaxf(alpha, 0.0f), 1.0f);
+    const float c[3] = {s0, s1, s2};
+    float nrgb[3];
+    calc_newrgb(c, ls_a, p.highpow, nrgb);
+    for (int i = 0; i < 3; ++i) {
+      const float perch = (1.0f - p.vibrancy) * 256.0f * powf(fmaxf(c[i] / 255.0f, 0.0f), g_inv);
+      const float bg = p.transparent ? 0.0f : (1.0f - alpha) * 256.0f * p.bg[i];
+      o[i] = fminf(fmaxf((nrgb[i] + perch + bg) / 256.0f, 0.0f), 1.0f);
+    }
+    o[3] = p.transparent ? alpha : 1.0f;
+  }
+  const size_t oi = (size_t)yi * p.width + xi;
+  if (kRgba8) {
+    uchar4 v;
+    v.x = (unsigned char)__float2int_rn(o[0] * 255.0f);
+    v.y = (unsigned char)__float2int_rn(o[1] * 255.0f);
+    v.z = (unsigned char)__float2int_rn(o[2] * 255.0f);
+    v.w = (unsigned char)__float2int_rn(o[3] * 255.0f);
+    ((uchar4*)out)[oi] = v;
+  } else {
+    ((float4*)out)[oi] = make_float4(o[0], o[1], o[2], o[3]);
+  }
+}
+
+// -------------------------------------------------------------- launch
+cudaError_t build_kw_table(const float* knorm, float* tab, cudaStream_t s) {
+  k_kw_table<<<kKwMaxR + 1, 256, 0, s>>>(knorm, tab);
+  return cudaGetLastError();
+}
+
+size_t kw_table_floats() { return (size_t)(kKwMaxR * (kKwMaxR + 1) * (2 * kKwMaxR + 1)) / 6 + kKwMaxR + 1 + 1; }
+
+cudaError_t launch_density(const uint32_t* hist, float* filtered, const DeParams& p,
+                           const float* knorm, const float* tab, cudaStream_t s) {
+  dim3 grid((p.width + kTile - 1) / kTile, (p.height + kTile - 1) / kTile);
+  k_density<<<grid, kDeThreads, 0, s>>>((const uint4*)hist, (float4*)filtered, p, knorm, tab);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, const TonemapParams& p,
+                           const float* kern, void* out, bool rgba8, cudaStream_t s) {
+  dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
+  if (hist_u32) {
+    if (rgba8) k_tonemap<true, true><<<grid, 256, 0, s>>>((const uint4*)hist_u32, nullptr, p, kern, out);
+    else k_tonemap<true, false><<<grid, 256, 0, s>>>((const uint4*)hist_u32, nullptr, p, kern, out);
+  } else {
+    if (rgba8) k_tonemap<false, true><<<grid, 256, 0, s>>>(nullptr, (const float4*)filtered, p, kern, out);
+    else k_tonemap<false, false><<<grid, 256, 0, s>>>(nullptr, (const float4*)filtered, p, kern, out);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace pyr3

@@ -1,0 +1,279 @@
+"""GPU parity: every stage of the CUDA path against the oracle, through the
+C-ABI (libpyr3cuda.so).
+
+* seeding, xform pick and the saturating scatter are bit-exact;
+* every implemented variation matches the reference's WGSL (compiled for the
+  CPU, oracle/_ref) on a seeded point grid within the f32 tolerance stated in
+  the test, and the flam3 f64 golden vectors;
+* density estimation + tonemap of an identical histogram agree within 1/255
+  per channel;
+* whole renders agree statistically with the reference's own chaos loop at
+  equal sample count.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pyr3_b200 import _lib, genome as G, renderer as R, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def _impl_ids():
+    out = []
+    for i in range(326):
+        impl, dc = C.c_int32(), C.c_int32()
+        nm = C.c_char_p()
+        _lib.check(_lib.lib().pyr3_variation_info(i, C.byref(impl), C.byref(dc), C.byref(nm)))
+        if impl.value:
+            out.append((i, nm.value.decode(), bool(dc.value)))
+    return out
+
+
+# ------------------------------------------------------------------ seeding
+@pytest.mark.parametrize("base", [0, 2_000_000, 3_391_000, 40_000_000])
+def test_seed_walkers_bit_exact(base):
+    """Device ISAAC seeding == packIsaacStates (src/isaac.ts:194), including
+    walker indices where the JS double product rounds (w >= 3393281)."""
+    n = 4096
+    dev = np.zeros(n * 36, np.uint32)
+    _lib.check(_lib.lib().pyr3_seed_walkers(1234567, base, n, _lib.ptr(dev)))
+    assert np.array_equal(dev, O.pack_isaac_states(n, 1234567, base))
+
+
+# --------------------------------------------------------------------- pick
+@pytest.mark.parametrize("n,xaos", [(1, False), (3, False), (12, True), (20, False), (128, True)])
+def test_pick_stream_bit_exact(n, xaos):
+    rng = np.random.default_rng(n)
+    w = rng.uniform(0.0, 1.0, n).astype(np.float32)
+    xa = rng.uniform(0.0, 2.0, (n, n)).astype(np.float32) if xaos else None
+    cnt = 200_000
+    prev = rng.integers(-1, n, cnt).astype(np.int32)
+    draws = rng.integers(0, 2 ** 32, cnt, dtype=np.uint64).astype(np.uint32)
+    out = np.zeros(cnt, np.uint32)
+    _lib.check(_lib.lib().pyr3_pick_stream(n, _lib.ptr(w), _lib.ptr(xa) if xa is not None else None,
+                                           cnt, _lib.ptr(prev), _lib.ptr(draws), _lib.ptr(out)))
+    rows = O.pack_xform_distrib(w.astype(np.float64), None if xa is None else xa.astype(np.float64))
+    assert np.array_equal(out, O.pick_stream(n, rows, prev, draws))
+
+
+# -------------------------------------------------------------------- splat
+@pytest.mark.parametrize("pal_mode,rot,agg", [(0, 0.0, 0), (1, 0.0, 0), (0, 0.7, 0), (1, 1.3, 1), (0, 0.0, 1)])
+def test_splat_bit_exact(pal_mode, rot, agg):
+    rng = np.random.default_rng(7 + pal_mode)
+    W, H = 97, 61
+    n = 300_000
+    pts = np.empty((n, 4), np.float32)
+    pts[:, 0] = rng.normal(0.0, 0.6, n)
+    pts[:, 1] = rng.normal(0.0, 0.6, n)
+    pts[:, 2] = rng.uniform(-0.2, 1.2, n)  # colour outside [0,1] is clamped
+    pts[:, 3] = rng.choice([1.0, 0.5, 0.0, 0.3], n)
+    pts[: n // 10, :2] = 0.01  # a hot bucket for the aggregation path
+    pal = rng.random(1024).astype(np.float32)
+    dev = np.zeros(W * H * 4, np.uint32)
+    _lib.check(_lib.lib().pyr3_splat_points(n, _lib.ptr(pts), W, H, 40.0, 0.1, -0.05, rot, pal_mode,
+                                            _lib.ptr(pal), agg, _lib.ptr(dev)))
+    ref = O.splat_points(pts, W, H, 40.0, 0.1, -0.05, rot, pal_mode, pal)
+    assert np.array_equal(dev, ref)
+
+
+def test_splat_saturation_bit_exact():
+    """src/chaos-saturate.gpu.test.ts: near-full cells pin at 2^32-1."""
+    W, H = 8, 8
+    pal = np.ones(1024, np.float32)
+    start = np.full(W * H * 4, 0xFFFFF000, np.uint32)
+    start[::7] = 5
+    n = 50_000
+    pts = np.zeros((n, 4), np.float32)
+    rng = np.random.default_rng(3)
+    pts[:, 0] = rng.uniform(-0.5, 0.5, n)
+    pts[:, 1] = rng.uniform(-0.5, 0.5, n)
+    pts[:, 2] = 0.5
+    pts[:, 3] = 1.0
+    for agg in (0, 1):
+        dev = start.copy()
+        _lib.check(_lib.lib().pyr3_splat_points(n, _lib.ptr(pts), W, H, 8.0, 0.0, 0.0, 0.0, 0,
+                                                _lib.ptr(pal), agg, _lib.ptr(dev)))
+        ref = O.splat_points(pts, W, H, 8.0, 0.0, 0.0, 0.0, 0, pal, start.copy())
+        assert np.array_equal(dev, ref)
+        assert (dev == 0xFFFFFFFF).sum() > 0
+
+
+# --------------------------------------------------------------- variations
+def _grid(n, rng):
+    pts = np.empty((n, 2), np.float32)
+    pts[:, 0] = rng.uniform(-2.0, 2.0, n)
+    pts[:, 1] = rng.uniform(-2.0, 2.0, n)
+    pts[:8] = [[0.5, 0.5], [-0.3, 0.9], [1.5, -0.2], [0.01, 0.02], [-1.1, -1.3], [2.0, 0.0],
+               [0.0, 1.0], [0.25, -0.75]]
+    return pts
+
+
+def _params(idx, rng):
+    cat = G.catalog()[idx]
+    p = np.zeros(10, np.float32)
+    for k, rg in enumerate(cat["ranges"][:10]):
+        if rg:
+            lo, hi, dflt = rg
+            p[k] = dflt if rng.random() < 0.5 else rng.uniform(lo, hi)
+    return p
+
+
+def _eval_dev(idx, pts, w, p, a0, a1, isaac):
+    out = np.zeros_like(pts)
+    st = isaac.copy()
+    _lib.check(_lib.lib().pyr3_eval_variation(idx, len(pts), _lib.ptr(pts), w, _lib.ptr(p),
+                                              _lib.ptr(a0), _lib.ptr(a1), _lib.ptr(st),
+                                              _lib.ptr(out)))
+    return out, st
+
+
+def _relerr(a, b):
+    scale = np.maximum(np.maximum(np.abs(a), np.abs(b)), 1.0)
+    d = np.abs(a.astype(np.float64) - b.astype(np.float64)) / scale
+    both_nan = np.isnan(a) & np.isnan(b)
+    both_inf = np.isinf(a) & np.isinf(b) & (np.sign(a) == np.sign(b))
+    d[both_nan | both_inf] = 0.0
+    d[np.isnan(d)] = np.inf
+    return d
+
+
+@pytest.mark.parametrize("case", _impl_ids(), ids=lambda c: c[1])
+def test_variation_matches_reference(case):
+    """CUDA variation vs the reference's WGSL (f32, CPU) on a seeded grid:
+    relative error (scale max(|a|,|b|,1)) <= 1e-3 on at least 99% of points
+    and the RNG streams consume identically (same ISAAC state afterwards)."""
+    idx, name, _ = case
+    rng = np.random.default_rng(idx + 11)
+    pts = _grid(512, rng)
+    p = _params(idx, rng)
+    a0 = np.array([0.8, -0.4, 0.1, 1.0], np.float32)
+    a1 = np.array([0.3, 0.5, 0.2, 1.0], np.float32)
+    isaac = O.pack_isaac_states(len(pts), 1000 + idx)
+    dev, st_dev = _eval_dev(idx, pts, 0.75, p, a0, a1, isaac)
+    st_ref = isaac.copy()
+    ref = O.ref_eval_grid(idx, pts, 0.75, p, a0, a1, st_ref)
+    err = np.maximum(_relerr(dev[:, 0], ref[:, 0]), _relerr(dev[:, 1], ref[:, 1]))
+    frac_ok = float((err <= 1e-3).mean())
+    assert frac_ok >= 0.99, (name, frac_ok, float(np.nanmax(err)))
+    same_draws = (st_dev.reshape(-1, 36)[:, 0] == st_ref.reshape(-1, 36)[:, 0]).mean()
+    assert same_draws >= 0.99, (name, same_draws)
+
+
+def test_variations_match_flam3_goldens():
+    import json
+    import os
+
+    fx = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "variations_flam3.json")))
+    impl = {i for i, _, _ in _impl_ids()}
+    loose = {"popcorn2": 2e-3}
+    bad = []
+    for f in fx:
+        if f["runner"] == "smoke" or f["idx"] not in impl:
+            continue
+        af = f["affine"]
+        a0 = np.array([af.get("a", 1), af.get("b", 0), af.get("c", 0), 1], np.float32)
+        a1 = np.array([af.get("d", 0), af.get("e", 1), af.get("f", 0), 1], np.float32)
+        p = np.array(f["params"], np.float32)
+        rows = np.array(f["rows"])
+        tries = 48 if f["runner"] in ("branch", "julia") else 1
+        best = np.full(len(rows), np.inf)
+        for t in range(tries):
+            pts = rows[:, :2].astype(np.float32)
+            isaac = O.pack_isaac_states(len(rows), 500 + t)
+            out = np.zeros_like(pts)
+            for w in np.unique(rows[:, 2]):
+                sel = rows[:, 2] == w
+                o, _ = _eval_dev(f["idx"], np.ascontiguousarray(pts[sel]), float(w), p, a0, a1,
+                                 np.ascontiguousarray(isaac.reshape(-1, 36)[sel].reshape(-1)))
+                out[sel] = o
+            err = np.maximum(np.abs(out[:, 0] - rows[:, 3]), np.abs(out[:, 1] - rows[:, 4]))
+            err = err / np.maximum(1.0, np.maximum(np.abs(rows[:, 3]), np.abs(rows[:, 4])))
+            best = np.minimum(best, err)
+        tol = loose.get(f["name"], 1e-4)
+        if (best > tol).any():
+            bad.append((f["name"], float(best.max())))
+    assert not bad, bad
+
+
+# ---------------------------------------------------- density + tonemap
+def _c1_histogram(W, H, iters=3000, walkers=1024, seed=5):
+    g = workloads.plain_small()
+    g.scale = W / 4
+    xf = G.pack_xforms(g)
+    pal = G.bake_lut(g.palette)
+    distrib = O.pack_xform_distrib([x.weight for x in g.xforms])
+    u = np.zeros(31, np.uint32)
+    f = u.view(np.float32)
+    i32 = u.view(np.int32)
+    u[0], u[1], u[2], u[3] = W, H, iters, 200
+    f[4], f[5], f[6] = g.scale, 0.0, 0.0
+    u[7] = seed
+    i32[8] = -1
+    u[12] = walkers
+    f[13] = 1e-7
+    hist = np.zeros(W * H * 4, np.uint32)
+    O.ref_chaos_run(u, xf, len(g.xforms), pal, distrib, O.pack_isaac_states(walkers, seed), 0,
+                    walkers, hist, 16)
+    return g, pal, hist, walkers * iters
+
+
+@pytest.mark.parametrize("os_,de", [(1, True), (2, True), (1, False), (2, False)])
+def test_density_tonemap_within_1_255(os_, de):
+    W, H = 160, 120
+    g, _, hist, samples = _c1_histogram(W * os_, H * os_)
+    g.scale = W / 4
+    p = R.Renderer.present_opts(None, g, force_de_off=not de)
+    out = np.zeros(W * H * 4, np.float32)
+    filt = np.zeros(W * os_ * H * os_ * 4, np.float32)
+    _lib.check(_lib.lib().pyr3_density_tonemap(_lib.ptr(hist), W, H, os_, 0.5, C.byref(p), samples,
+                                               _lib.ptr(out), _lib.ptr(filt)))
+    k1, k2 = O.derive_calibration(g.scale, samples, 4.0, os_)
+    kern = O.spatial_kernel(0.5, os_)
+    src = {}
+    if de:
+        src["src_f32"] = O.density(hist, W * os_, H * os_, 9.0 * os_ + 1, 0.0 * os_ + 1, 0.4,
+                                   np.float32(k1), np.float32(k2))
+        rel = np.abs(filt - src["src_f32"]) / np.maximum(np.abs(src["src_f32"]), 1e-3)
+        assert float(np.percentile(rel, 99.9)) < 1e-4
+    else:
+        src["src_u32"] = hist
+    ref = O.visualize(W, H, os_, kern, np.float32(k1), np.float32(k2), 4.0, 1.0, 1.0, 0.01, **src)
+    assert float(np.abs(out - ref).max()) <= 1.0 / 255.0
+
+
+# ---------------------------------------------------- whole-render statistics
+def _collapse(hist, W, H, os_):
+    h = hist.reshape(H * os_, W * os_, 4).astype(np.float64)
+    return h.reshape(H, os_, W, os_, 4).sum(axis=(1, 3))
+
+
+def test_whole_render_statistical_parity():
+    """C1 genome on a 320x240 canvas: the CUDA renderer (its own walker pool)
+    vs the reference's chaos_main on the CPU (1024 walkers), equal sample
+    count.  Log-density relative L1 <= 1% and tonemapped PSNR >= 40 dB."""
+    W, H = 320, 240
+    walkers, iters = 1024, 48_000
+    g, pal, ref_hist, samples = _c1_histogram(W, H, iters=iters, walkers=walkers, seed=9)
+    r = R.create_renderer(W, H, 1)
+    r.reset(g)
+    r.iterate(g, seed=77, walkers=walkers, iters_per_walker=iters)
+    s, _ = r.counters()
+    assert s == samples
+    dev_hist, _, _ = r.read_histogram()
+    a = np.log1p(_collapse(dev_hist.reshape(-1), W, H, 1)[..., 3] / 255.0)
+    b = np.log1p(_collapse(ref_hist, W, H, 1)[..., 3] / 255.0)
+    l1 = float(np.abs(a - b).sum() / b.sum())
+    img_dev = r.present(g, samples, fmt="f32").astype(np.float64)
+    k1, k2 = O.derive_calibration(g.scale, samples, 4.0, 1)
+    ref_img = O.ref_density(ref_hist, W, H, 10.0, 1.0, 0.4, np.float32(k1), np.float32(k2))
+    ref_img = O.visualize(W, H, 1, O.spatial_kernel(0.5, 1), np.float32(k1), np.float32(k2), 4.0, 1.0,
+                          1.0, 0.01, src_f32=ref_img).reshape(H, W, 4)
+    mse = float(((img_dev[..., :3] - ref_img[..., :3]) ** 2).mean())
+    psnr = 10 * np.log10(1.0 / max(mse, 1e-20))
+    print(f"log-density L1 {l1:.4%}  PSNR {psnr:.2f} dB")
+    assert l1 <= 0.01
+    assert psnr >= 40.0
+    r.destroy()
