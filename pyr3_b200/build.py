@@ -56,6 +56,9 @@ def generate_sources() -> str:
     unknown = (impl | dcs) - set(names)
     if unknown:
         raise RuntimeError(f"variation library defines names not in the catalog: {sorted(unknown)}")
+    perm = json.load(open(os.path.join(PKG, "catalog.json")))["perlin_perm"]
+    core += ("\n__device__ const unsigned char c_perlin_perm[256] = {" +
+             ", ".join(str(v) for v in perm) + "};\n")
     out = ["// generated by pyr3_b200/build.py -- do not edit"]
     out.append(f"static const char* const kSrcCore = {_raw(core)};")
     out.append(f"static const int kNumVlib = {len(vsrc)};")

@@ -111,7 +111,13 @@ def generate(ref_root: str) -> dict:
             "ranges": prange,
             "dc": i in dc,
         })
-    return {"count": len(out), "variations": out}
+    # Ken Perlin's improved-noise permutation as the reference's dc_perlin
+    # uses it (src/shaders/noise_perlin.wgsl:12, 256 entries repeated).
+    ptxt = open(os.path.join(src, "shaders", "noise_perlin.wgsl")).read()
+    a = ptxt.index("array<u32, 512>(")
+    perm = [int(x) for x in re.findall(r"(\d+)u", ptxt[a:ptxt.index(");", a)])]
+    assert len(perm) == 512 and perm[:256] == perm[256:]
+    return {"count": len(out), "variations": out, "perlin_perm": perm[:256]}
 
 
 if __name__ == "__main__":

@@ -228,7 +228,7 @@ static std::string shape_one(const float* X, XformShape* s) {
     float fi = X[20 + 4 * j];
     if (!(fi >= 0.0f) || !std::isfinite(fi)) return "variation index is not a non-negative number";
     int idx = (int)fi;
-    if (idx == 97 || (idx >= 0 && idx < kNumVariations && kVarImpl[idx])) {
+    if (idx == 97 || variation_implemented(idx) || variation_is_dc(idx)) {
       s->vars.push_back(idx);
     } else if (idx >= kNumVariations) {
       s->vars.push_back(-1);  // the reference's default case contributes (0, 0)

@@ -87,7 +87,8 @@ VDEV void isaac_mix8(u32* v) {
 
 VDEV u32 walker_hash(u64 w) {
   if (w < (1ull << 21)) return (u32)w * 2654435761u + 1u;
-  double d = (double)w * 2654435761.0 + 1.0;  // exact below 2^53, JS rounding above
+  // JS evaluates the product and the sum as two rounded doubles: no FMA.
+  double d = __dadd_rn(__dmul_rn((double)w, 2654435761.0), 1.0);
   u64 q = (u64)d;
   return (u32)(q & 0xffffffffull);
 }
@@ -169,24 +170,32 @@ VDEV float3 mix3(float3 a, float3 b, float t) {
   return make_float3(wmix(a.x, b.x, t), wmix(a.y, b.y, t), wmix(a.z, b.z, t));
 }
 
+// Palette mix a*(1-t) + b*t with separately rounded products (no FMA), so
+// the fixed-point deposit is bit-identical to the reference arithmetic.
+VDEV float mix_rn(float a, float b, float t) {
+  return __fadd_rn(__fmul_rn(a, __fsub_rn(1.0f, t)), __fmul_rn(b, t));
+}
+
 VDEV void splat(const ChaosArgs& A, const float4* pal, float3 sp, float2 p_start, float opacity,
                 int dc_hit, float3 dc, u64* n_in) {
-  float dx = sp.x - A.cx, dy = sp.y - A.cy;
-  float rx = dx * A.cos_r - dy * A.sin_r;
-  float ry = dx * A.sin_r + dy * A.cos_r;
-  float px = rx * A.scale + (float)A.width * 0.5f;
-  float py = ry * A.scale + (float)A.height * 0.5f;
+  // Bucket coordinates (chaos.wgsl:8575-8585), every product and sum rounded
+  // on its own so the floor() boundaries match the reference exactly.
+  float dx = __fsub_rn(sp.x, A.cx), dy = __fsub_rn(sp.y, A.cy);
+  float rx = __fsub_rn(__fmul_rn(dx, A.cos_r), __fmul_rn(dy, A.sin_r));
+  float ry = __fadd_rn(__fmul_rn(dx, A.sin_r), __fmul_rn(dy, A.cos_r));
+  float px = __fadd_rn(__fmul_rn(rx, A.scale), __fmul_rn((float)A.width, 0.5f));
+  float py = __fadd_rn(__fmul_rn(ry, A.scale), __fmul_rn((float)A.height, 0.5f));
   i32 xi = f2i(floorf(px)), yi = f2i(floorf(py));
   if (!(xi >= 0 && xi < (i32)A.width && yi >= 0 && yi < (i32)A.height)) return;
   *n_in += 1;
-  float cxf = wclamp(sp.z, 0.0f, 1.0f) * 255.0f;
+  float cxf = __fmul_rn(wclamp(sp.z, 0.0f, 1.0f), 255.0f);
   float4 pc;
   if (A.palette_mode == 1u) {
     u32 i0 = f2u(cxf);
-    float fr = cxf - (float)i0;
+    float fr = __fsub_rn(cxf, (float)i0);
     if (i0 >= 255u) { i0 = 254u; fr = 1.0f; }
     float4 a = pal[i0], b = pal[i0 + 1];
-    pc = make_float4(wmix(a.x, b.x, fr), wmix(a.y, b.y, fr), wmix(a.z, b.z, fr), wmix(a.w, b.w, fr));
+    pc = make_float4(mix_rn(a.x, b.x, fr), mix_rn(a.y, b.y, fr), mix_rn(a.z, b.z, fr), mix_rn(a.w, b.w, fr));
   } else {
     pc = pal[min(f2u(cxf), 255u)];
   }
@@ -216,9 +225,10 @@ VDEV void splat(const ChaosArgs& A, const float4* pal, float3 sp, float2 p_start
       rgb = mix3(rgb, hsv_rgb(hue, 1.0f, wmix(1.0f, 0.5f, ring)), wclamp(A.phase_strength, 0.0f, 1.0f));
     }
   }
-  float wgt = opacity * 255.0f;
+  float wgt = __fmul_rn(opacity, 255.0f);
   u32* cell = A.hist + ((u64)yi * A.width + (u32)xi) * 4u;
-  u32 dr = f2u(rgb.x * wgt), dg = f2u(rgb.y * wgt), db = f2u(rgb.z * wgt), dn = f2u(wgt);
+  u32 dr = f2u(__fmul_rn(rgb.x, wgt)), dg = f2u(__fmul_rn(rgb.y, wgt)), db = f2u(__fmul_rn(rgb.z, wgt));
+  u32 dn = f2u(wgt);
 #if AGGREGATE
   // Warp-aggregate identical buckets: one atomic per distinct cell.
   const u32 act = __activemask();
@@ -237,7 +247,7 @@ VDEV void splat(const ChaosArgs& A, const float4* pal, float3 sp, float2 p_start
     add_sat(cell + 3, dn);
   }
   if (A.capture_index && A.idx_sum) {
-    add_sat(A.idx_sum + (u64)yi * A.width + (u32)xi, f2u(wclamp(sp.z, 0.0f, 1.0f) * wgt));
+    add_sat(A.idx_sum + (u64)yi * A.width + (u32)xi, f2u(__fmul_rn(wclamp(sp.z, 0.0f, 1.0f), wgt)));
   }
 }
 
