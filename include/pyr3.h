@@ -78,7 +78,8 @@ typedef struct {
  * total walkers*iters but spreads it over its own persistent walker pool
  * (each stream still seeded by the reference's packIsaacStates rule). */
 #define PYR3_ITER_EXACT_WALKERS 1u
-/* Warp-aggregate identical histogram buckets with __match_any_sync. */
+/* Pool every distinct histogram bucket of a warp (__match_any_sync) instead
+   of only the warp's hot bucket. */
 #define PYR3_ITER_AGGREGATE 2u
 
 /* present() request (src/renderer.ts:148-158, visualize.ts:178-204). */

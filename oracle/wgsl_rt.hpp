@@ -238,9 +238,13 @@ template <class T> inline T fsel(float f, double d) { return std::is_same_v<T, f
 #define WG_F1(NAME, EXPR)                                                  \
   template <class A> inline auto NAME(const A &a) {                        \
     return map1([](auto x) { using T = decltype(x); (void)sizeof(T); return EXPR; }, a); }
-WG_F1(sin, (T)std::sin(x))
-WG_F1(cos, (T)std::cos(x))
-WG_F1(tan, (T)std::tan(x))
+// sin / cos / tan of an f32 are the correctly rounded f32 value (evaluated
+// in f64, rounded once).  WGSL leaves their accuracy to the implementation;
+// this fixes one canonical answer, and the hash-style variations
+// (fract(sin(.) * 43758.5453)) depend on every bit of it.
+WG_F1(sin, (T)std::sin((double)x))
+WG_F1(cos, (T)std::cos((double)x))
+WG_F1(tan, (T)std::tan((double)x))
 WG_F1(asin, (T)std::asin(x))
 WG_F1(acos, (T)std::acos(x))
 WG_F1(atan, (T)std::atan(x))

@@ -93,7 +93,9 @@ VDEV u32 walker_hash(u64 w) {
   return (u32)(q & 0xffffffffull);
 }
 
-VDEV void seed_walker(const Rng& r, u32 seed, u64 w) {
+// Out of line: once per walker, and large once unrolled.
+OUTL void seed_walker_at(u32* s, u32 W, u32 seed, u64 w) {
+  const Rng r{s, W};
   u32 pcg = seed ^ walker_hash(w);
 #pragma unroll
   for (int k = 0; k < 4; ++k) pcg = pcg * 747796405u + 2891336453u;
@@ -133,6 +135,7 @@ VDEV void seed_walker(const Rng& r, u32 seed, u64 w) {
   isaac_round(r);
   r.f(0) = 16u;
 }
+VDEV void seed_walker(const Rng& r, u32 seed, u64 w) { seed_walker_at(r.s, r.W, seed, w); }
 
 // -------------------------------------------------------------- xform pick
 // Row r of the reference's table (src/genome.ts:482-534) is nondecreasing
@@ -229,18 +232,44 @@ VDEV void splat(const ChaosArgs& A, const float4* pal, float3 sp, float2 p_start
   u32* cell = A.hist + ((u64)yi * A.width + (u32)xi) * 4u;
   u32 dr = f2u(__fmul_rn(rgb.x, wgt)), dg = f2u(__fmul_rn(rgb.y, wgt)), db = f2u(__fmul_rn(rgb.z, wgt));
   u32 dn = f2u(wgt);
-#if AGGREGATE
-  // Warp-aggregate identical buckets: one atomic per distinct cell.
+  // Warp aggregation.  Lanes whose deltas are below 2^26 may pool them (a
+  // sum over 32 lanes then stays below 2^31, so pooling never wraps and the
+  // saturating result min(total, 2^32 - 1) is unchanged).
+  const u32 lane = threadIdx.x & 31u;
   const u32 act = __activemask();
   const u32 key = (u32)yi * A.width + (u32)xi;
-  const u32 peers = __match_any_sync(act, key);
-  dr = __reduce_add_sync(peers, dr);
-  dg = __reduce_add_sync(peers, dg);
-  db = __reduce_add_sync(peers, db);
-  dn = __reduce_add_sync(peers, dn);
-  if ((threadIdx.x & 31u) == (u32)(__ffs(peers) - 1))
+  const bool small = ((dr | dg | db | dn) >> 26) == 0u;
+  bool deposit = true;
+#if AGGREGATE
+  // Every distinct bucket of the warp deposits once (__match_any_sync).
+  const u32 peers = __match_any_sync(act, small ? key : (0x80000000u | lane));
+  if (__popc(peers) > 1) {
+    dr = __reduce_add_sync(peers, dr);
+    dg = __reduce_add_sync(peers, dg);
+    db = __reduce_add_sync(peers, db);
+    dn = __reduce_add_sync(peers, dn);
+    deposit = lane == (u32)(__ffs(peers) - 1);
+  }
+#else
+  // The hot bucket: lanes that hit the first eligible lane's bucket pool
+  // their deltas.  Costs a shuffle and two ballots; turns the same-cell
+  // atomic storm of a collapsing attractor into one deposit per warp.
+  const u32 ok = __ballot_sync(act, small);
+  if (ok) {
+    const int lead = __ffs(ok) - 1;
+    const u32 k0 = __shfl_sync(act, key, lead);
+    const bool mine = small && key == k0;
+    const u32 grp = __ballot_sync(act, mine);
+    if (mine && __popc(grp) > 1) {
+      dr = __reduce_add_sync(grp, dr);
+      dg = __reduce_add_sync(grp, dg);
+      db = __reduce_add_sync(grp, db);
+      dn = __reduce_add_sync(grp, dn);
+      deposit = lane == (u32)lead;
+    }
+  }
 #endif
-  {
+  if (deposit) {
     add_sat(cell + 0, dr);
     add_sat(cell + 1, dg);
     add_sat(cell + 2, db);

@@ -22,6 +22,57 @@ typedef unsigned long long u64;
 
 #define VDEV __device__ __forceinline__
 
+// --------------------------------------------------- out-of-line libm
+// CUDA's accurate transcendental paths are long; inlined at every call site
+// of every variation they made one genome's specialised kernel larger than
+// the SM instruction cache.  Each is compiled once here and called; the
+// names below redirect the library (and the kernel) to these copies.  The
+// values are the same functions' values.
+#define OUTL __device__ __noinline__
+OUTL float ol_sinf(float x) { return sinf(x); }
+OUTL float ol_cosf(float x) { return cosf(x); }
+OUTL float2 ol_sincos(float x) {
+  float s, c;
+  sincosf(x, &s, &c);
+  return make_float2(s, c);
+}
+OUTL float ol_tanf(float x) { return tanf(x); }
+OUTL float ol_expf(float x) { return expf(x); }
+OUTL float ol_logf(float x) { return logf(x); }
+OUTL float ol_log2f(float x) { return log2f(x); }
+OUTL float ol_log10f(float x) { return log10f(x); }
+OUTL float ol_powf(float x, float y) { return powf(x, y); }
+OUTL float ol_atan2f(float y, float x) { return atan2f(y, x); }
+OUTL float ol_atanf(float x) { return atanf(x); }
+OUTL float ol_asinf(float x) { return asinf(x); }
+OUTL float ol_acosf(float x) { return acosf(x); }
+OUTL float ol_sinhf(float x) { return sinhf(x); }
+OUTL float ol_coshf(float x) { return coshf(x); }
+OUTL float ol_tanhf(float x) { return tanhf(x); }
+OUTL float ol_asinhf(float x) { return asinhf(x); }
+OUTL float ol_acoshf(float x) { return acoshf(x); }
+OUTL float ol_atanhf(float x) { return atanhf(x); }
+OUTL double ol_sin(double x) { return sin(x); }
+#define sinf ol_sinf
+#define cosf ol_cosf
+#define tanf ol_tanf
+#define expf ol_expf
+#define logf ol_logf
+#define log2f ol_log2f
+#define log10f ol_log10f
+#define powf ol_powf
+#define atan2f ol_atan2f
+#define atanf ol_atanf
+#define asinf ol_asinf
+#define acosf ol_acosf
+#define sinhf ol_sinhf
+#define coshf ol_coshf
+#define tanhf ol_tanhf
+#define asinhf ol_asinhf
+#define acoshf ol_acoshf
+#define atanhf ol_atanhf
+#define sin ol_sin
+
 #define P_PI 3.14159265358979323846f
 #define P_TAU 6.28318530717958647692f
 #define P_HALF_PI 1.57079632679489661923f
@@ -41,6 +92,13 @@ VDEV float2& operator+=(float2& a, float2 b) { a.x += b.x; a.y += b.y; return a;
 VDEV float dot2(float2 a, float2 b) { return a.x * b.x + a.y * b.y; }
 VDEV float sq2(float2 a) { return a.x * a.x + a.y * a.y; }
 VDEV float len2(float2 a) { return sqrtf(a.x * a.x + a.y * a.y); }
+// Separately rounded products, for expressions whose outcome hinges on the
+// last bit (a branch on a near-zero discriminant, a hash of a product, an
+// angle of 1e5 rad): the compiler never fuses an __fmul_rn into an add, so
+// these round exactly as the reference's f32 operations do.
+VDEV float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+VDEV float dot_rn(float ax, float ay, float bx, float by) { return mul_rn(ax, bx) + mul_rn(ay, by); }
+VDEV float len_rn(float x, float y) { return sqrtf(mul_rn(x, x) + mul_rn(y, y)); }
 
 // ------------------------------------------------------- WGSL semantics
 VDEV float wpow(float x, float y) {
@@ -79,15 +137,15 @@ VDEV float hash01(u32 h) {
   h ^= h >> 15;
   return (float)h * (1.0f / 4294967296.0f);
 }
-VDEV float ssin(float a) {
-  return fabsf(a) <= 1.0e6f ? sinf(a) : sinf(hash01(__float_as_uint(a)) * P_TAU);
+VDEV float safe_arg(float a) {  // |a| > 1e6: trig of a hash of the bits
+  return fabsf(a) <= 1.0e6f ? a : hash01(__float_as_uint(a)) * P_TAU;
 }
-VDEV float scos(float a) {
-  return fabsf(a) <= 1.0e6f ? cosf(a) : cosf(hash01(__float_as_uint(a)) * P_TAU);
-}
+VDEV float ssin(float a) { return sinf(safe_arg(a)); }
+VDEV float scos(float a) { return cosf(safe_arg(a)); }
 VDEV void ssincos(float a, float* s, float* c) {
-  float t = fabsf(a) <= 1.0e6f ? a : hash01(__float_as_uint(a)) * P_TAU;
-  sincosf(t, s, c);
+  float2 r = ol_sincos(safe_arg(a));
+  *s = r.x;
+  *c = r.y;
 }
 VDEV float stan(float a) { return ssin(a) / scos(a); }
 VDEV float stanh(float a) { return tanhf(wclamp(a, -20.0f, 20.0f)); }
@@ -107,12 +165,14 @@ struct Rng {
   VDEV u32& f(u32 k) const { return s[k * W]; }
 };
 
-// One ISAAC round (Jenkins' isaac() with RANDSIZL = 4), flam3 isaac.c.
-VDEV void isaac_round(const Rng& r) {
-  u32 a = r.f(1);
-  u32 c = r.f(3) + 1u;
-  r.f(3) = c;
-  u32 b = r.f(2) + c;
+// One ISAAC round (Jenkins' isaac() with RANDSIZL = 4), flam3 isaac.c,
+// on the state at s (fields W words apart).  Out of line: it runs once per
+// sixteen draws, and inlined at every draw site it dominated the code size.
+OUTL void isaac_round_at(u32* s, u32 W) {
+  u32 a = s[1 * W];
+  u32 c = s[3 * W] + 1u;
+  s[3 * W] = c;
+  u32 b = s[2 * W] + c;
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     const int m = i, m2 = (i + 8) & 15;
@@ -123,16 +183,17 @@ VDEV void isaac_round(const Rng& r) {
       case 2: mixed = a ^ (a << 2); break;
       default: mixed = a ^ (a >> 16); break;
     }
-    u32 x = r.f(4 + m);
-    a = mixed + r.f(4 + m2);
-    u32 y = r.f(4 + ((x >> 2) & 15u)) + a + b;
-    r.f(4 + m) = y;
-    b = r.f(4 + ((y >> 6) & 15u)) + x;
-    r.f(20 + m) = b;
+    u32 x = s[(4 + m) * W];
+    a = mixed + s[(4 + m2) * W];
+    u32 y = s[(4 + ((x >> 2) & 15u)) * W] + a + b;
+    s[(4 + m) * W] = y;
+    b = s[(4 + ((y >> 6) & 15u)) * W] + x;
+    s[(20 + m) * W] = b;
   }
-  r.f(1) = a;
-  r.f(2) = b;
+  s[1 * W] = a;
+  s[2 * W] = b;
 }
+VDEV void isaac_round(const Rng& r) { isaac_round_at(r.s, r.W); }
 
 VDEV u32 irand(const Rng& r) {
   u32 cnt = r.f(0);

@@ -124,17 +124,25 @@ VAR(checks) {  // P = x, y, size, rnd
   else { dx = P[0]; dy = P[1] + rny; }
   return f2(w * (p.x + dx), w * (p.y + dy));
 }
+// fract(sin(k . p + seed) * 43758.5453) amplifies one ulp of the sine by
+// 4e4: the argument is separately rounded and the sine is the correctly
+// rounded f32 value (double sine rounded once), as the reference's f32 ops.
+VDEV float circ_hash(float x, float y, float kx, float ky, float seed) {
+  float a = mul_rn(x, kx) + mul_rn(y, ky) + seed;
+  float ar = mul_rn((float)sin((double)a), 43758.5453f);
+  return ar - truncf(ar);
+}
 VAR(circular) {  // P = angle, seed
   float ca = P[0] * P_PI / 180.0f;
-  float ar = sinf(p.x * 12.9898f + p.y * 78.233f + P[1]) * 43758.5453f;
-  float rnd = (2.0f * (RAND01() + (ar - truncf(ar))) - 2.0f) * ca;
+  float aux = circ_hash(p.x, p.y, 12.9898f, 78.233f, P[1]);
+  float rnd = (2.0f * (RAND01() + aux) - 2.0f) * ca;
   float rad = sqrtf(p.x * p.x + p.y * p.y), ang = atan2f(p.y, p.x);
   return f2(w * cosf(ang + rnd) * rad, w * sinf(ang + rnd) * rad);
 }
 VAR(circular2) {  // P = angle, seed, x, y
   float ca = P[0] * P_PI / 180.0f;
-  float ar = sinf(p.x * P[2] + p.y * P[3] + P[1]) * 43758.5453f;
-  float rnd = (2.0f * (RAND01() + (ar - truncf(ar))) - 2.0f) * ca;
+  float aux = circ_hash(p.x, p.y, P[2], P[3], P[1]);
+  float rnd = (2.0f * (RAND01() + aux) - 2.0f) * ca;
   float rad = sqrtf(p.x * p.x + p.y * p.y), ang = atan2f(p.y, p.x);
   return f2(w * cosf(ang + rnd) * rad, w * sinf(ang + rnd) * rad);
 }
@@ -250,7 +258,8 @@ VAR(phoenix_julia) {  // P = power, dist, x_distort, y_distort
   float pw = P[0] == 0.0f ? 1.0f : P[0];
   float px = p.x * (P[2] + 1.0f), py = p.y * (P[3] + 1.0f);
   float k = floorf(RAND01() * 32768.0f);
-  float a = atan2f(py, px) * (P[1] / pw) + k * (2.0f * P_PI / pw);
+  // |a| reaches 1e5 rad: separately rounded products keep its last bit.
+  float a = mul_rn(atan2f(py, px), P[1] / pw) + mul_rn(k, 2.0f * P_PI / pw);
   return polar2(w * wpow(fmaxf(p.x * p.x + p.y * p.y, 1e-30f), P[1] / (2.0f * pw)), a);
 }
 VAR(unpolar) {

@@ -4,15 +4,20 @@
 // 5971-6516.
 #pragma once
 
+// Chaotic billiards (chaos.wgsl:5971-6280).  A walker outside the table is
+// projected onto its rim, so the ray-circle discriminants below sit next to
+// zero and the hit branch turns on their last bit: every product that feeds
+// a sum is separately rounded (mul_rn), as the reference's f32 ops are.
 // Specular reflection of unit direction v at hit point h with normal n,
 // continuing the remaining path length.
 VDEV float2 billiard_bounce(float2 h, float vx, float vy, float nx, float ny, float rest) {
-  float d = vx * nx + vy * ny;
-  return f2(h.x + rest * (vx - 2.0f * d * nx), h.y + rest * (vy - 2.0f * d * ny));
+  float d = dot_rn(vx, vy, nx, ny);
+  float rx = vx - mul_rn(2.0f * d, nx), ry = vy - mul_rn(2.0f * d, ny);
+  return f2(h.x + mul_rn(rest, rx), h.y + mul_rn(rest, ry));
 }
 VAR(billiard_circle) {  // P = radius, step, angle
   float rc = fmaxf(P[0], 1.0e-5f), step = P[1];
-  float px = p.x, py = p.y, r0 = len2(p);
+  float px = p.x, py = p.y, r0 = len_rn(p.x, p.y);
   if (r0 > rc) {
     px = (px / r0) * rc;
     py = (py / r0) * rc;
@@ -22,13 +27,13 @@ VAR(billiard_circle) {  // P = radius, step, angle
   if (r0 > 1.0e-6f) { bx = px / r0; by = py / r0; }
   float sa, ca;
   ssincos(P[2], &sa, &ca);
-  float vx = bx * ca - by * sa, vy = bx * sa + by * ca;
-  float dp = px * vx + py * vy;
-  float disc = dp * dp + rc * rc - (px * px + py * py);
+  float vx = mul_rn(bx, ca) - mul_rn(by, sa), vy = mul_rn(bx, sa) + mul_rn(by, ca);
+  float dp = dot_rn(px, py, vx, vy);
+  float disc = mul_rn(dp, dp) + mul_rn(rc, rc) - dot_rn(px, py, px, py);
   float th = -dp + sqrtf(fmaxf(disc, 0.0f));
-  float fx = px + step * vx, fy = py + step * vy;
+  float fx = px + mul_rn(step, vx), fy = py + mul_rn(step, vy);
   if (th > 0.0f && th < step) {
-    float2 h = f2(px + th * vx, py + th * vy);
+    float2 h = f2(px + mul_rn(th, vx), py + mul_rn(th, vy));
     float2 q = billiard_bounce(h, vx, vy, -h.x / rc, -h.y / rc, step - th);
     fx = q.x;
     fy = q.y;
@@ -40,9 +45,9 @@ VAR(billiard_stadium) {  // P = width, height, step, angle
   float px = p.x, py = p.y;
   if (fabsf(px) > w2) {
     float cx = px > 0.0f ? w2 : -w2, dx = px - cx;
-    float dist = len2(f2(dx, py));
+    float dist = len_rn(dx, py);
     if (dist > R) {
-      px = cx + (dx / dist) * R;
+      px = cx + mul_rn(dx / dist, R);
       py = (py / dist) * R;
     }
   } else if (fabsf(py) > R) {
@@ -53,35 +58,35 @@ VAR(billiard_stadium) {  // P = width, height, step, angle
   float th = 1.0e10f;
   int wall = 0;
   if (vy > 0.0f) {
-    float t = (R - py) / vy, x = px + t * vx;
+    float t = (R - py) / vy, x = px + mul_rn(t, vx);
     if (t >= 0.0f && x >= -w2 && x <= w2 && t < th) { th = t; wall = 1; }
   }
   if (vy < 0.0f) {
-    float t = (-R - py) / vy, x = px + t * vx;
+    float t = (-R - py) / vy, x = px + mul_rn(t, vx);
     if (t >= 0.0f && x >= -w2 && x <= w2 && t < th) { th = t; wall = 2; }
   }
   for (int side = 0; side < 2; ++side) {  // right then left cap
     float dx = side == 0 ? px - w2 : px + w2;
-    float dp = dx * vx + py * vy;
-    float disc = dp * dp + R * R - (dx * dx + py * py);
+    float dp = dot_rn(dx, py, vx, vy);
+    float disc = mul_rn(dp, dp) + mul_rn(R, R) - dot_rn(dx, py, dx, py);
     if (disc >= 0.0f) {
-      float t = -dp + sqrtf(disc), x = px + t * vx;
+      float t = -dp + sqrtf(disc), x = px + mul_rn(t, vx);
       bool ok = side == 0 ? x >= w2 - 1.0e-5f : x <= -w2 + 1.0e-5f;
       if (t >= 0.0f && ok && t < th) { th = t; wall = 3 + side; }
     }
   }
-  float fx = px + step * vx, fy = py + step * vy;
+  float fx = px + mul_rn(step, vx), fy = py + mul_rn(step, vy);
   if (th > 0.0f && th < step) {
-    float2 h = f2(px + th * vx, py + th * vy);
+    float2 h = f2(px + mul_rn(th, vx), py + mul_rn(th, vy));
     float nx = 0.0f, ny = 0.0f;
     if (wall == 1) ny = -1.0f;
     else if (wall == 2) ny = 1.0f;
     else if (wall == 3) {
-      float rl = fmaxf(len2(f2(h.x - w2, h.y)), 1.0e-5f);
+      float rl = fmaxf(len_rn(h.x - w2, h.y), 1.0e-5f);
       nx = -(h.x - w2) / rl;
       ny = -h.y / rl;
     } else if (wall == 4) {
-      float rl = fmaxf(len2(f2(h.x + w2, h.y)), 1.0e-5f);
+      float rl = fmaxf(len_rn(h.x + w2, h.y), 1.0e-5f);
       nx = -(h.x + w2) / rl;
       ny = -h.y / rl;
     }
@@ -96,7 +101,7 @@ VAR(billiard_sinai) {  // P = length, radius, step, angle
   float px = p.x, py = p.y;
   if (fabsf(px) > L2) px = px > 0.0f ? L2 : -L2;
   if (fabsf(py) > L2) py = py > 0.0f ? L2 : -L2;
-  float r0 = len2(f2(px, py));
+  float r0 = len_rn(px, py);
   if (r0 < R) {
     if (r0 > 1.0e-6f) {
       px = (px / r0) * R;
@@ -112,32 +117,32 @@ VAR(billiard_sinai) {  // P = length, radius, step, angle
   float th = 1.0e10f;
   int wall = 0;
   if (vx < 0.0f) {
-    float t = (-L2 - px) / vx, y = py + t * vy;
+    float t = (-L2 - px) / vx, y = py + mul_rn(t, vy);
     if (t >= 0.0f && y >= -L2 && y <= L2 && t < th) { th = t; wall = 1; }
   }
   if (vx > 0.0f) {
-    float t = (L2 - px) / vx, y = py + t * vy;
+    float t = (L2 - px) / vx, y = py + mul_rn(t, vy);
     if (t >= 0.0f && y >= -L2 && y <= L2 && t < th) { th = t; wall = 2; }
   }
   if (vy < 0.0f) {
-    float t = (-L2 - py) / vy, x = px + t * vx;
+    float t = (-L2 - py) / vy, x = px + mul_rn(t, vx);
     if (t >= 0.0f && x >= -L2 && x <= L2 && t < th) { th = t; wall = 3; }
   }
   if (vy > 0.0f) {
-    float t = (L2 - py) / vy, x = px + t * vx;
+    float t = (L2 - py) / vy, x = px + mul_rn(t, vx);
     if (t >= 0.0f && x >= -L2 && x <= L2 && t < th) { th = t; wall = 4; }
   }
   {
-    float dp = px * vx + py * vy;
-    float disc = dp * dp - ((px * px + py * py) - R * R);
+    float dp = dot_rn(px, py, vx, vy);
+    float disc = mul_rn(dp, dp) - (dot_rn(px, py, px, py) - mul_rn(R, R));
     if (disc >= 0.0f) {
       float t = -dp - sqrtf(disc);
       if (t >= 0.0f && t < th) { th = t; wall = 5; }
     }
   }
-  float fx = px + step * vx, fy = py + step * vy;
+  float fx = px + mul_rn(step, vx), fy = py + mul_rn(step, vy);
   if (th > 0.0f && th < step) {
-    float2 h = f2(px + th * vx, py + th * vy);
+    float2 h = f2(px + mul_rn(th, vx), py + mul_rn(th, vy));
     float nx = 0.0f, ny = 0.0f;
     if (wall == 1) nx = 1.0f;
     else if (wall == 2) nx = -1.0f;
@@ -155,7 +160,7 @@ VAR(billiard_polygon) {  // P = sides, radius, step, angle
   const float R = fmaxf(P[1], 1.0e-5f), step = P[2];
   const float inr = R * cosf(3.141592653589793f / (float)sides);
   float px = p.x, py = p.y;
-  float r0 = len2(f2(px, py));
+  float r0 = len_rn(px, py);
   if (r0 > inr) {
     float s = inr / fmaxf(r0, 1.0e-6f);
     px *= s;
@@ -170,25 +175,25 @@ VAR(billiard_polygon) {  // P = sides, radius, step, angle
     float ph = (2.0f * 3.141592653589793f * (float)(k + 1u)) / (float)sides;
     float bx = R * scos(ph), by = R * ssin(ph);
     float dx = bx - ax, dy = by - ay;
-    float det = -vx * dy + vy * dx;
+    float det = mul_rn(-vx, dy) + mul_rn(vy, dx);
     if (fabsf(det) > 1.0e-6f) {
-      float t = (-(ax - px) * dy + (ay - py) * dx) / det;
-      float u = (vx * (ay - py) - vy * (ax - px)) / det;
+      float t = (mul_rn(-(ax - px), dy) + mul_rn(ay - py, dx)) / det;
+      float u = (mul_rn(vx, ay - py) - mul_rn(vy, ax - px)) / det;
       if (t >= 0.0f && u >= 0.0f && u <= 1.0f && t < th) { th = t; seg = (i32)k; }
     }
     ax = bx;
     ay = by;
   }
-  float fx = px + step * vx, fy = py + step * vy;
+  float fx = px + mul_rn(step, vx), fy = py + mul_rn(step, vy);
   if (th > 0.0f && th < step && seg != -1) {
-    float2 h = f2(px + th * vx, py + th * vy);
+    float2 h = f2(px + mul_rn(th, vx), py + mul_rn(th, vy));
     float p0 = (2.0f * 3.141592653589793f * (float)seg) / (float)sides;
     float p1 = (2.0f * 3.141592653589793f * (float)(seg + 1)) / (float)sides;
     float a0x = R * scos(p0), a0y = R * ssin(p0), b0x = R * scos(p1), b0y = R * ssin(p1);
     float ex = b0x - a0x, ey = b0y - a0y;
-    float el = fmaxf(len2(f2(ex, ey)), 1.0e-5f);
+    float el = fmaxf(len_rn(ex, ey), 1.0e-5f);
     float nx = -ey / el, ny = ex / el;
-    if (nx * (0.5f * (a0x + b0x)) + ny * (0.5f * (a0y + b0y)) > 0.0f) { nx = -nx; ny = -ny; }
+    if (dot_rn(nx, ny, 0.5f * (a0x + b0x), 0.5f * (a0y + b0y)) > 0.0f) { nx = -nx; ny = -ny; }
     float2 q = billiard_bounce(h, vx, vy, nx, ny, step - th);
     fx = q.x;
     fy = q.y;
