@@ -190,6 +190,9 @@ def bench_ours(args, ws, rank, local, dist):
     W, H = g.size
     os_ = g.oversample
     walkers, iters, samples = R.compute_dispatch(g.quality, W, H)
+    if args.samples:  # profiling case: same genome and canvas, fewer samples per step
+        walkers, iters = 1024, max(1, args.samples // 1024)
+        samples = walkers * iters
     r = R.create_renderer(W, H, os_, g.filter_radius, device=local)
     gg = R.GpuGenome(g)
     r.prepare(gg)  # NVRTC specialisation (cached), outside the timed region
@@ -323,6 +326,8 @@ def main():
     ap.add_argument("--config", default="headline", choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--samples", type=int, default=0,
+                    help="override samples per step (small profiling case; not a bench number)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     ws, rank, local, dist = _dist()
