@@ -179,6 +179,24 @@ int pyr3_splat_points(uint32_t n, const float *pts, uint32_t width, uint32_t hei
 int pyr3_density_tonemap(const uint32_t *hist, uint32_t width, uint32_t height,
                          uint32_t oversample, float filter_radius, const pyr3_present_opts *p,
                          uint64_t total_samples, float *out_rgba, float *filtered_out);
+/* Allocation-free density estimation + tonemap.  No counterpart in the
+ * reference: it is for callers that cannot allocate device memory -- code
+ * inside another engine's frame loop or memory pool, or code that must not
+ * allocate once running.  The caller passes a super-res histogram already
+ * on the device (superW x superH x 4 u32) and a device output image
+ * (width x height, PYR3_OUT_RGBA8 or PYR3_OUT_RGBA32F); the intermediate
+ * density output and lookup tables live in one fixed array inside the
+ * library (about 16.4 MiB, held by every GPU that loads the library until
+ * the process exits).  Limit: width*height*oversample^2 <= 1,048,576
+ * super-sampled pixels, larger canvases fail with PYR3_E_INVALID.  Runs on
+ * `stream` (a cudaStream_t, NULL = default stream) of the current device.
+ * The first call on a device sets the array up synchronously, so make it
+ * before any stream capture.  All calls share the array: calls whose GPU
+ * work overlaps race and must be serialised by the caller. */
+int pyr3_density_tonemap_noalloc(const uint32_t *device_hist, uint32_t width, uint32_t height,
+                                 uint32_t oversample, float filter_radius,
+                                 const pyr3_present_opts *p, uint64_t total_samples,
+                                 void *device_out, int32_t out_kind, void *stream);
 /* Compile (or fetch from cache) the chaos kernel for a genome structure;
  * returns the NVRTC log on failure via pyr3_last_error. */
 int pyr3_prepare(pyr3_renderer *r, const pyr3_genome *g);

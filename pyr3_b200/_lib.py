@@ -96,6 +96,9 @@ _SIGS = {
                                     C.c_int32, C.c_void_p]),
     "pyr3_density_tonemap": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
                                        C.POINTER(PresentOpts), C.c_uint64, C.c_void_p, C.c_void_p]),
+    "pyr3_density_tonemap_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                               C.c_float, C.POINTER(PresentOpts), C.c_uint64,
+                                               C.c_void_p, C.c_int32, C.c_void_p]),
     "pyr3_prepare": (C.c_int, [C.c_void_p, C.POINTER(GenomeC)]),
     "pyr3_jit_compile": (C.c_int, [C.POINTER(GenomeC), C.c_int32, C.POINTER(C.c_uint64)]),
     "pyr3_jit_source": (C.c_int, [C.POINTER(GenomeC), C.c_char_p, C.c_uint64, C.POINTER(C.c_uint64)]),

@@ -5,7 +5,8 @@
    implements, found by scanning the VAR(...) / DCV(...) definitions) into
    csrc/gen/jit_sources.inc.
 2. nvcc -gencode arch=compute_100a,code=sm_100a the C-ABI (capi.cpp), the
-   JIT driver (jit.cpp) and the density / tonemap passes (passes.cu).
+   JIT driver (jit.cpp), the density / tonemap passes (passes.cu) and the
+   fixed scratch of the allocation-free present (noalloc.cu).
 """
 from __future__ import annotations
 
@@ -81,9 +82,9 @@ def generate_sources() -> str:
 
 def build(force: bool = False) -> str:
     inc = generate_sources()
-    srcs = [os.path.join(CSRC, f) for f in ("capi.cpp", "jit.cpp", "passes.cu")]
+    srcs = [os.path.join(CSRC, f) for f in ("capi.cpp", "jit.cpp", "passes.cu", "noalloc.cu")]
     deps = srcs + [inc, os.path.join(ROOT, "include", "pyr3.h"), os.path.join(CSRC, "jit.h"),
-                   os.path.join(CSRC, "passes.h")]
+                   os.path.join(CSRC, "passes.h"), os.path.join(CSRC, "noalloc.h")]
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
         return LIB
     cmd = [NVCC, "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

@@ -6,10 +6,12 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "jit.h"
+#include "noalloc.h"
 #include "passes.h"
 #include "pyr3.h"
 
@@ -761,6 +763,75 @@ PYR3_API int pyr3_density_tonemap(const uint32_t* hist, uint32_t width, uint32_t
   if (rc) return rc;
   if (filtered_out && p->density_on)
     CUDA_TRY(cudaMemcpy(filtered_out, r->d_filtered, (size_t)r->SW * r->SH * 16, cudaMemcpyDeviceToHost));
+  return PYR3_OK;
+}
+
+// ------------------------------------------------ allocation-free present
+// Density estimation + tonemap of a histogram the caller already holds on
+// the device, into an image on the device, for callers that cannot
+// allocate device memory (see noalloc.cu).  Same kernels and parameters as
+// pyr3_present; the renderer-owned buffers are replaced by the library's
+// fixed scratch array.
+PYR3_API int pyr3_density_tonemap_noalloc(const uint32_t* device_hist, uint32_t width,
+                                          uint32_t height, uint32_t oversample,
+                                          float filter_radius, const pyr3_present_opts* p,
+                                          uint64_t total_samples, void* device_out,
+                                          int32_t out_kind, void* stream) {
+  if (!device_hist || !p || !device_out || oversample == 0 || width == 0 || height == 0)
+    return fail(PYR3_E_INVALID, "bad arguments");
+  if (out_kind != PYR3_OUT_RGBA8 && out_kind != PYR3_OUT_RGBA32F)
+    return fail(PYR3_E_INVALID, "unknown output kind");
+  if (total_samples == 0) return fail(PYR3_E_INVALID, "total_samples must be positive");
+  const uint64_t sw = (uint64_t)width * oversample, sh = (uint64_t)height * oversample;
+  if (sw * sh > pyr3::kNoAllocMaxSuperPixels)
+    return fail(PYR3_E_INVALID,
+                "canvas too large for the allocation-free present: width*height*oversample^2 = " +
+                    std::to_string(sw * sh) + " exceeds its fixed scratch of " +
+                    std::to_string(pyr3::kNoAllocMaxSuperPixels) + " super-sampled pixels");
+  cudaStream_t s = (cudaStream_t)stream;
+  static float knorm[257];
+  static std::once_flag knorm_once;
+  std::call_once(knorm_once, [] { kernel_norm_lut(knorm); });
+  pyr3::NoAllocScratch sc;
+  CUDA_TRY(pyr3::noalloc_scratch(knorm, s, &sc));
+  float taps[pyr3::kMaxTaps];
+  const int fwidth = spatial_kernel(filter_radius > 0 ? filter_radius : 0.5f, (int)oversample, taps);
+  CUDA_TRY(cudaMemcpyAsync(sc.kern, taps, (size_t)fwidth * sizeof(float), cudaMemcpyHostToDevice, s));
+  // src/calibration.ts:37-43 in double, uploaded as f32.
+  const double os2 = (double)oversample * (double)oversample;
+  const float k1 = (float)((p->brightness * 255.0 * 268.0) / 256.0);
+  const float k2 = (float)((os2 * p->scale * p->scale) / (255.0 * (double)total_samples));
+  const float* filtered = nullptr;
+  if (p->density_on) {
+    pyr3::DeParams d;
+    d.width = (uint32_t)sw;
+    d.height = (uint32_t)sh;
+    d.max_rad = (float)((double)p->de_max_rad * oversample + 1.0);
+    d.min_rad = (float)((double)p->de_min_rad * oversample + 1.0);
+    d.curve = p->de_curve;
+    d.k1 = k1;
+    d.k2 = k2;
+    d.R = (int)std::ceil(std::min(std::max(d.max_rad, 0.0f), 256.0f));
+    CUDA_TRY(pyr3::launch_density(device_hist, sc.filtered, d, sc.knorm, sc.kwtab, s));
+    filtered = sc.filtered;
+  }
+  pyr3::TonemapParams t;
+  t.width = width;
+  t.height = height;
+  t.oversample = oversample;
+  t.fwidth = (uint32_t)fwidth;
+  t.k1 = k1;
+  t.k2 = k2;
+  t.gamma = p->gamma;
+  t.vibrancy = p->vibrancy;
+  t.highpow = p->highpow;
+  t.linrange = p->linrange;
+  t.bg[0] = p->background[0];
+  t.bg[1] = p->background[1];
+  t.bg[2] = p->background[2];
+  t.transparent = p->transparent;
+  CUDA_TRY(pyr3::launch_tonemap(filtered ? nullptr : device_hist, filtered, t, sc.kern, device_out,
+                                out_kind == PYR3_OUT_RGBA8, s));
   return PYR3_OK;
 }
 
