@@ -81,6 +81,15 @@ typedef struct {
 /* Pool every distinct histogram bucket of a warp (__match_any_sync) instead
    of only the warp's hot bucket. */
 #define PYR3_ITER_AGGREGATE 2u
+/* Chaos kernel.  Without either flag an autotuner picks, per genome
+ * structure, the faster of the two on the first launch of at least 2^26
+ * samples (that launch then waits for its trial runs), and smaller launches
+ * before that use the barrier kernel.  The barrier kernel runs each round of
+ * a CTA's walkers in xform order between barriers; the queue kernel (genomes
+ * of up to 32 xforms) keeps per-xform walker queues so warps run one xform
+ * at a time without barriers. */
+#define PYR3_ITER_KERNEL_BARRIER 4u
+#define PYR3_ITER_KERNEL_QUEUE 8u
 
 /* present() request (src/renderer.ts:148-158, visualize.ts:178-204). */
 typedef struct {

@@ -24,6 +24,8 @@ OUT_RGBA8 = 0
 OUT_RGBA32F = 1
 ITER_EXACT_WALKERS = 1
 ITER_AGGREGATE = 2
+ITER_KERNEL_BARRIER = 4
+ITER_KERNEL_QUEUE = 8
 
 
 class Pyr3Error(RuntimeError):

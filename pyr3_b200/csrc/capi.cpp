@@ -42,6 +42,8 @@ constexpr uint32_t kGrain = 16384;
 constexpr uint32_t kFuse = 200;         // src/renderer.ts:41
 constexpr float kDefaultJitter = 1e-7f; // src/chaos.ts:96
 constexpr int kWpb = 256;
+// Launches of at least this many samples may run the kernel autotuner.
+constexpr uint64_t kTuneMinSamples = 64ull << 20;
 
 // Host mirror of the NVRTC kernel's argument block (layout must match
 // ChaosArgs in csrc/jit/chaos_kernel.cuh).
@@ -66,6 +68,9 @@ struct ChaosArgs {
   float phase_strength, phase_freq;
   float xform_blend;
   uint64_t* counters;
+  uint64_t* sched;
+  uint32_t* wrec;
+  uint32_t cta_slots;
 };
 
 // ---- host restatements of the reference's host-side math --------------
@@ -184,9 +189,13 @@ struct pyr3_renderer {
   uint16_t* d_pick = nullptr;
   size_t pick_cap = 0;
   uint64_t* d_counters = nullptr;
+  uint64_t* d_sched = nullptr;  // queue kernel: [0] walkers handed out, [1] sticky fault flags
+  uint32_t* d_wrec = nullptr;   // queue kernel: walker records (CTAs x slots)
+  size_t wrec_cap = 0;
   bool capture = false;
   float last_ms = 0.0f;
   cudaEvent_t marks[8] = {};
+  cudaEvent_t tune[3] = {};  // kernel autotuner
   void* d_flush = nullptr;
   size_t flush_bytes = 0;
   std::vector<std::shared_ptr<pyr3::ChaosModule>> modules;  // keep-alive
@@ -262,6 +271,7 @@ PYR3_API int pyr3_create(const pyr3_opts* opts, pyr3_renderer** out) {
   CUDA_TRY(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreate(&r->ev0));
   CUDA_TRY(cudaEventCreate(&r->ev1));
+  for (auto& e : r->tune) CUDA_TRY(cudaEventCreate(&e));
   CUDA_TRY(cudaMalloc(&r->d_pal, 1024 * 4));
   CUDA_TRY(cudaMemsetAsync(r->d_pal, 0, 1024 * 4, r->stream));
   CUDA_TRY(cudaMalloc(&r->d_knorm, 257 * 4));
@@ -269,6 +279,8 @@ PYR3_API int pyr3_create(const pyr3_opts* opts, pyr3_renderer** out) {
   CUDA_TRY(cudaMalloc(&r->d_kern, pyr3::kMaxTaps * 4));
   CUDA_TRY(cudaMalloc(&r->d_counters, 16));
   CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, 16, r->stream));
+  CUDA_TRY(cudaMalloc(&r->d_sched, 16));
+  CUDA_TRY(cudaMemsetAsync(r->d_sched, 0, 16, r->stream));
   float knorm[257];
   kernel_norm_lut(knorm);
   CUDA_TRY(cudaMemcpyAsync(r->d_knorm, knorm, sizeof knorm, cudaMemcpyHostToDevice, r->stream));
@@ -294,8 +306,12 @@ PYR3_API int pyr3_destroy(pyr3_renderer* r) {
   cudaFree(r->d_kern);
   cudaFree(r->d_pick);
   cudaFree(r->d_counters);
+  cudaFree(r->d_sched);
+  cudaFree(r->d_wrec);
   cudaFree(r->d_flush);
   for (auto& e : r->marks)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : r->tune)
     if (e) cudaEventDestroy(e);
   if (r->ev0) cudaEventDestroy(r->ev0);
   if (r->ev1) cudaEventDestroy(r->ev1);
@@ -325,6 +341,7 @@ PYR3_API int pyr3_reset(pyr3_renderer* r, const float* palette) {
   CUDA_TRY(cudaMemsetAsync(r->d_hist, 0, n * 16, r->stream));
   CUDA_TRY(cudaMemsetAsync(r->d_idx, 0, n * 4, r->stream));
   CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, 16, r->stream));
+  CUDA_TRY(cudaMemsetAsync(r->d_sched, 0, 16, r->stream));
   return PYR3_OK;
 }
 
@@ -356,6 +373,64 @@ PYR3_API int pyr3_prepare(pyr3_renderer* r, const pyr3_genome* g) {
   return prepare_module(r, g, false, &m);
 }
 
+namespace {
+// Launch one chaos kernel for `total` post-fuse samples on walkers
+// walker_base.. of this launch's seed: `walkers` of them (0: pool_walkers),
+// total / walkers iterations each plus one for the first total % walkers.
+// Returns the walkers used through *used.
+// Walkers a launch of `total` samples uses on one kernel: enough to fill
+// the machine, not so many that the per-walker burn-in dominates.
+uint64_t pool_walkers(pyr3_renderer* r, const pyr3::ChaosModule& m, bool queue, uint64_t total) {
+  const int sms = device_sms(r->device);
+  const uint64_t ctas = (uint64_t)(queue ? m.queue_blocks_per_sm : m.blocks_per_sm) * sms;
+  const uint64_t per_cta = queue ? (uint64_t)pyr3::kQueueSlots : (uint64_t)m.wpb;
+  const uint64_t want = std::max<uint64_t>((uint64_t)sms * 256u, total / (5ull * kFuse));
+  return std::max<uint64_t>(1, std::min<uint64_t>(ctas * per_cta, std::min<uint64_t>(want, total)));
+}
+
+int launch_chaos(pyr3_renderer* r, const pyr3::ChaosModule& m, bool queue, ChaosArgs A,
+                 uint64_t total, uint64_t walker_base, uint64_t walkers, uint64_t* used) {
+  const int sms = device_sms(r->device);
+  const uint64_t ctas = (uint64_t)(queue ? m.queue_blocks_per_sm : m.blocks_per_sm) * sms;
+  const uint64_t per_cta = queue ? (uint64_t)pyr3::kQueueSlots : (uint64_t)m.wpb;
+  const uint64_t nw = walkers ? walkers : pool_walkers(r, m, queue, total);
+  const uint64_t base = total / nw, extra = total % nw;
+  if (queue && base + 1 + kFuse > 0xffffffffull)
+    return fail(PYR3_E_INVALID, "too many iterations per walker for one launch (> 2^32)");
+  A.walker_base = walker_base;
+  A.n_walkers = nw;
+  A.iters_base = base;
+  A.iters_extra = extra;
+  void* params[] = {&A};
+  if (queue) {
+    // One persistent CTA per SM; each fills cta_slots of its slots first
+    // (fewer than all for small launches, so the walkers spread over every
+    // SM) and refills slots from sched[0] as walkers finish.
+    const size_t rec_bytes = (size_t)ctas * per_cta * pyr3::kWalkerRecordBytes;
+    if (rec_bytes > r->wrec_cap) {
+      CUDA_TRY(cudaStreamSynchronize(r->stream));
+      cudaFree(r->d_wrec);
+      r->d_wrec = nullptr;
+      r->wrec_cap = 0;
+      CUDA_TRY(cudaMalloc(&r->d_wrec, rec_bytes));
+      r->wrec_cap = rec_bytes;
+    }
+    uint64_t slots = (nw + ctas - 1) / ctas;
+    slots = std::min<uint64_t>(per_cta, (slots + 31) & ~31ull);
+    A.wrec = r->d_wrec;
+    A.cta_slots = (uint32_t)slots;
+    CUDA_TRY(cudaMemsetAsync(r->d_sched, 0, 8, r->stream));
+    LAUNCH_TRY(m.queue, (unsigned)ctas, (unsigned)(pyr3::kQueueWarps * 32), m.queue_smem, r->stream,
+               params);
+  } else {
+    const unsigned grid = (unsigned)std::min<uint64_t>((nw + m.wpb - 1) / m.wpb, ctas);
+    LAUNCH_TRY(m.chaos, grid, (unsigned)m.wpb, m.smem, r->stream, params);
+  }
+  *used = nw;
+  return PYR3_OK;
+}
+}  // namespace
+
 PYR3_API int pyr3_iterate(pyr3_renderer* r, const pyr3_genome* g, const pyr3_iterate_opts* o) {
   if (!r || !g || !o) return fail(PYR3_E_INVALID, "null argument");
   cudaSetDevice(r->device);
@@ -384,34 +459,14 @@ PYR3_API int pyr3_iterate(pyr3_renderer* r, const pyr3_genome* g, const pyr3_ite
   if (xf_bytes > m->c_xf_bytes) return fail(PYR3_E_INVALID, "xform records exceed module constant bank");
   CUDA_TRY(cudaMemcpyAsync(m->c_xf, g->xforms, xf_bytes, cudaMemcpyHostToDevice, r->stream));
 
-  // walker decomposition
   const uint64_t total = o->walkers * o->iters_per_walker;
   if (total == 0) return PYR3_OK;
-  uint64_t nw, base, extra;
-  const int sms = device_sms(r->device);
-  const uint64_t pool = (uint64_t)m->blocks_per_sm * sms * m->wpb;
-  if (o->flags & PYR3_ITER_EXACT_WALKERS) {
-    nw = o->walkers;
-    base = o->iters_per_walker;
-    extra = 0;
-  } else {
-    // Keep the sample total; use enough walkers to fill the machine, but
-    // not so many that the per-walker burn-in dominates.
-    uint64_t want = std::max<uint64_t>((uint64_t)sms * m->wpb, total / (5ull * kFuse));
-    nw = std::min<uint64_t>(pool, std::min<uint64_t>(want, total));
-    base = total / nw;
-    extra = total % nw;
-  }
   ChaosArgs A;
   std::memset(&A, 0, sizeof A);
   A.hist = r->d_hist;
   A.idx_sum = r->capture ? r->d_idx : nullptr;
   A.palette = r->d_pal;
   A.pick_start = r->d_pick;
-  A.walker_base = 0;
-  A.n_walkers = nw;
-  A.iters_base = base;
-  A.iters_extra = extra;
   A.fuse = kFuse;
   A.width = r->SW;
   A.height = r->SH;
@@ -443,12 +498,56 @@ PYR3_API int pyr3_iterate(pyr3_renderer* r, const pyr3_genome* g, const pyr3_ite
   A.phase_freq = o->phase_freq;
   A.xform_blend = std::min(1.0f, std::max(0.0f, g->xform_blend));
   A.counters = r->d_counters;
-  const uint64_t sets = (nw + m->wpb - 1) / m->wpb;
-  const uint64_t resident = (uint64_t)m->blocks_per_sm * sms;
-  const unsigned grid = (unsigned)std::min<uint64_t>(sets, resident);
-  void* params[] = {&A};
+  A.sched = r->d_sched;
+
+  const bool exact = (o->flags & PYR3_ITER_EXACT_WALKERS) != 0;
+  uint64_t done = 0, walker_base = 0, used = 0;
+  bool use_queue = false;
   CUDA_TRY(cudaEventRecord(r->ev0, r->stream));
-  LAUNCH_TRY(m->chaos, grid, (unsigned)m->wpb, m->smem, r->stream, params);
+  if (!m->queue || (o->flags & PYR3_ITER_KERNEL_BARRIER)) {
+    use_queue = false;
+  } else if (o->flags & PYR3_ITER_KERNEL_QUEUE) {
+    use_queue = true;
+  } else if (m->choice.load() >= 0) {
+    use_queue = m->choice.load() == 1;
+  } else if (!exact && total >= kTuneMinSamples) {
+    // Autotune: the first large launch of this genome structure runs a
+    // short trial on each chaos kernel -- with the walker count that kernel
+    // would use for the whole launch, so that the trial sees the same
+    // occupancy and queue lengths -- and the rest of the samples (and every
+    // later launch) on the kernel whose predicted time for the remaining
+    // samples, burn-in included, is lower.  Every sample still lands in the
+    // histogram; each launch uses fresh walker indices.
+    const uint64_t nw_b = pool_walkers(r, *m, false, total), nw_q = pool_walkers(r, *m, true, total);
+    const uint64_t t_b = nw_b * std::max<uint64_t>(1, total / 32 / nw_b);
+    const uint64_t t_q = nw_q * std::max<uint64_t>(1, total / 32 / nw_q);
+    float ms_b = 0.0f, ms_q = 0.0f;
+    CUDA_TRY(cudaEventRecord(r->tune[0], r->stream));
+    rc = launch_chaos(r, *m, false, A, t_b, 0, nw_b, &used);
+    if (rc) return rc;
+    walker_base += used;
+    CUDA_TRY(cudaEventRecord(r->tune[1], r->stream));
+    rc = launch_chaos(r, *m, true, A, t_q, walker_base, nw_q, &used);
+    if (rc) return rc;
+    walker_base += used;
+    CUDA_TRY(cudaEventRecord(r->tune[2], r->stream));
+    CUDA_TRY(cudaEventSynchronize(r->tune[2]));
+    CUDA_TRY(cudaEventElapsedTime(&ms_b, r->tune[0], r->tune[1]));
+    CUDA_TRY(cudaEventElapsedTime(&ms_q, r->tune[1], r->tune[2]));
+    done = t_b + t_q;
+    const double rest = (double)(total > done ? total - done : 0);
+    // ms per iteration (burn-in iterations included) times the iterations
+    // the rest of the launch needs on each kernel.
+    const double per_b = ms_b / ((double)t_b + (double)nw_b * kFuse);
+    const double per_q = ms_q / ((double)t_q + (double)nw_q * kFuse);
+    use_queue = per_q * (rest + (double)nw_q * kFuse) < per_b * (rest + (double)nw_b * kFuse);
+    m->choice.store(use_queue ? 1 : 0);
+  }
+  if (done < total) {
+    if (exact) rc = launch_chaos(r, *m, use_queue, A, total, 0, o->walkers, &used);
+    else rc = launch_chaos(r, *m, use_queue, A, total - done, walker_base, 0, &used);
+    if (rc) return rc;
+  }
   CUDA_TRY(cudaEventRecord(r->ev1, r->stream));
   return PYR3_OK;
 }
@@ -527,13 +626,24 @@ PYR3_API int pyr3_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t
   return PYR3_OK;
 }
 
+namespace {
+// The queue chaos kernel sets sched[1] if one of its bounded waits ran out
+// (a scheduling fault); it stays set until the next reset.
+int check_sched(pyr3_renderer* r) {
+  uint64_t f = 0;
+  CUDA_TRY(cudaMemcpyAsync(&f, r->d_sched + 1, 8, cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  if (f) return fail(PYR3_E_CUDA, "chaos kernel: a walker-queue wait exceeded its limit");
+  return PYR3_OK;
+}
+}  // namespace
+
 PYR3_API int pyr3_read_histogram(pyr3_renderer* r, uint32_t* host_out) {
   if (!r || !host_out) return fail(PYR3_E_INVALID, "null argument");
   cudaSetDevice(r->device);
   CUDA_TRY(cudaMemcpyAsync(host_out, r->d_hist, (size_t)r->SW * r->SH * 16, cudaMemcpyDeviceToHost,
                            r->stream));
-  CUDA_TRY(cudaStreamSynchronize(r->stream));
-  return PYR3_OK;
+  return check_sched(r);
 }
 
 PYR3_API int pyr3_read_index_map(pyr3_renderer* r, uint32_t* host_out) {
@@ -548,8 +658,7 @@ PYR3_API int pyr3_read_index_map(pyr3_renderer* r, uint32_t* host_out) {
 PYR3_API int pyr3_sync(pyr3_renderer* r) {
   if (!r) return fail(PYR3_E_INVALID, "null renderer");
   cudaSetDevice(r->device);
-  CUDA_TRY(cudaStreamSynchronize(r->stream));
-  return PYR3_OK;
+  return check_sched(r);
 }
 
 PYR3_API int pyr3_info(pyr3_renderer* r, uint32_t* super_w, uint32_t* super_h, void** device_hist) {
@@ -565,7 +674,8 @@ PYR3_API int pyr3_counters(pyr3_renderer* r, uint64_t* samples, uint64_t* splats
   uint64_t c[2] = {0, 0};
   cudaSetDevice(r->device);
   CUDA_TRY(cudaMemcpyAsync(c, r->d_counters, 16, cudaMemcpyDeviceToHost, r->stream));
-  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  int rc = check_sched(r);
+  if (rc) return rc;
   if (samples) *samples = c[0];
   if (splats) *splats = c[1];
   return PYR3_OK;

@@ -166,12 +166,19 @@ std::string gen_chain(const XformShape& x, const std::string& base, const char* 
   return o.str();
 }
 
+}  // namespace
+
+bool use_queue(int nxf) { return nxf >= 1 && nxf <= kQueueMaxXforms; }
+
+namespace {
+
 std::string gen_chaos_source(const GenomeShape& s, int wpb, bool aggregate) {
   const int nxf = (int)s.xf.size();
   std::ostringstream o;
   o << "#define NXF " << nxf << "\n#define WPB " << wpb << "\n#define HAS_FINAL "
     << (s.has_final ? 1 : 0) << "\n#define FINAL_SLOT " << nxf << "\n#define PICK_LINEAR "
-    << (nxf <= 16 ? 1 : 0) << "\n#define AGGREGATE " << (aggregate ? 1 : 0) << "\n";
+    << (nxf <= 16 ? 1 : 0) << "\n#define AGGREGATE " << (aggregate ? 1 : 0) << "\n#define QUEUE "
+    << (use_queue(nxf) ? 1 : 0) << "\n#define QWARPS " << kQueueWarps << "\n";
   o << library_source() << "\n";
   o << kSrcChaosPre << "\n";
   o << "VDEV void xform_chain(int k, float2 p, float pz, Ctx& c, ChainOut& o) {\n  switch (k) {\n";
@@ -305,6 +312,24 @@ int get_chaos_module(const GenomeShape& s, int wpb, bool aggregate,
   if (cr != cudaSuccess || nb < 1) {
     *err = "chaos kernel cannot be resident (shared memory / registers)";
     return PYR3_E_CUDA;
+  }
+  if (use_queue(nxf)) {
+    // Shared memory of the queue kernel (chaos_kernel.cuh, QUEUE): palette,
+    // one staging area per warp, rings [NXF][QP] u16, pick boundaries,
+    // heads, tails, live counter, current ring.
+    if (cudaLibraryGetKernel(&m->queue, m->mod, "chaos_queue_kernel") != cudaSuccess) {
+      *err = "chaos module is missing chaos_queue_kernel";
+      return PYR3_E_CUDA;
+    }
+    m->queue_smem = 256 * 16 + (size_t)kQueueWarps * kQueueStageWords * 4 +
+                    (size_t)nxf * kQueueSlots * 2 + pick_u16 * 2 + (size_t)nxf * 8 + 8;
+    cudaFuncSetAttribute((const void*)m->queue, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)m->queue_smem);
+    int qb = 0;
+    cr = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&qb, (const void*)m->queue, kQueueWarps * 32,
+                                                       m->queue_smem);
+    if (cr == cudaSuccess && qb >= 1) m->queue_blocks_per_sm = qb;
+    else m->queue = nullptr;  // not resident: the barrier kernel serves this structure
   }
   m->blocks_per_sm = nb;
   {

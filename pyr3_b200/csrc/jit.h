@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <atomic>
 #include <memory>
 #include <string>
 #include <vector>
@@ -12,6 +13,16 @@ namespace pyr3 {
 constexpr int kXformFloats = 116;
 constexpr int kMaxVars = 8;
 constexpr int kNumVariations = 326;
+// Queue chaos kernel (genomes of up to kQueueMaxXforms xforms): one CTA of
+// kQueueWarps warps per SM owning kQueueSlots walkers, whose records
+// (kWalkerRecordBytes each) live in global memory; each warp stages
+// kQueueStageWords u32 in shared memory, next to one ring per xform.
+constexpr int kQueueMaxXforms = 32;
+constexpr int kQueueWarps = 16;
+constexpr int kQueueSlots = 2048;
+constexpr int kQueueStageWords = 36 * 33 + 7 * 32;
+constexpr int kWalkerRecordBytes = 192;
+bool use_queue(int nxf);
 
 // The part of a genome that changes the generated code: how many xforms,
 // which variations each one sums (in slot order), which have a post
@@ -45,6 +56,13 @@ struct ChaosModule {
   int wpb = 256;
   size_t smem = 0;      // dynamic shared memory of chaos_kernel
   int blocks_per_sm = 1;
+  // chaos_queue_kernel (genomes of <= kQueueMaxXforms xforms), else null.
+  cudaKernel_t queue = nullptr;
+  size_t queue_smem = 0;
+  int queue_blocks_per_sm = 0;
+  // Kernel choice of the autotuner for this structure: -1 not measured
+  // yet, 0 chaos_kernel, 1 chaos_queue_kernel.
+  std::atomic<int> choice{-1};
   ~ChaosModule();
 };
 

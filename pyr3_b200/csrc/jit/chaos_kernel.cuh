@@ -66,6 +66,9 @@ struct ChaosArgs {
   float phase_strength, phase_freq;
   float xform_blend;
   u64* counters;           // [0] accepted samples, [1] splats in bounds
+  u64* sched;              // queue kernel: [0] walkers handed out, [1] fault flags
+  u32* wrec;               // queue kernel: gridDim.x x QP walker records, 48 u32 each
+  u32 cta_slots;           // queue kernel: slots filled per CTA at the start (<= QP)
 };
 
 // ---------------------------------------------------------------- seeding
@@ -283,6 +286,84 @@ VDEV void splat(const ChaosArgs& A, const float4* pal, float3 sp, float2 p_start
 // ==== PYR3 KERNEL SECTION ====
 // (the generator inserts xform_chain / final_chain above this line)
 
+#ifndef QUEUE
+#define QUEUE 0
+#endif
+
+// One xform chain of walker state p0/pz for xform k, with the optional
+// xform blend (chaos.wgsl:8372-8381): with probability xform_blend a
+// second xform's chain is mixed in.
+VDEV void run_chain(const ChaosArgs& A, const unsigned short* pst, int k, float2 p0, float pz,
+                    const Rng& rng, ChainOut& o) {
+  Ctx cx;
+  cx.rng = rng;
+  const float* X = c_xf + k * 116;
+  cx.a0 = make_float4(X[0], X[1], X[2], X[3]);
+  cx.a1 = make_float4(X[4], X[5], X[6], X[7]);
+  o.dc_hit = 0;
+  o.dc = make_float3(0.0f, 0.0f, 0.0f);
+  xform_chain(k, p0, pz, cx, o);
+  if (A.xform_blend > 0.0f) {
+    if (rand01(rng) < A.xform_blend) {
+      u32 bi = pick_xform(pst, NXF, irand(rng) & 16383u);
+      Ctx cb = cx;
+      const float* XB = c_xf + bi * 116;
+      cb.a0 = make_float4(XB[0], XB[1], XB[2], XB[3]);
+      cb.a1 = make_float4(XB[4], XB[5], XB[6], XB[7]);
+      ChainOut ob;
+      ob.dc_hit = 0;
+      ob.dc = make_float3(0.0f, 0.0f, 0.0f);
+      xform_chain((int)bi, p0, pz, cb, ob);
+      float tb = rand01(rng);
+      o.pv = f2(wmix(o.pv.x, ob.pv.x, tb), wmix(o.pv.y, ob.pv.y, tb));
+      o.nz = wmix(o.nz, ob.nz, tb);
+    }
+  }
+}
+
+VDEV bool bad_point(float2 v) {  // chaos.wgsl:8391: NaN or |v| > 1e10
+  return (v.x != v.x) || (v.y != v.y) || fabsf(v.x) > 1e10f || fabsf(v.y) > 1e10f;
+}
+
+// Accepted iteration (chaos.wgsl:8455-8730) after the chain of xform fn
+// produced pv / nz: final xform behind its opacity gate, scale-relative
+// jitter of the walker position, and the splat once past the fuse.
+// Returns the walker's next position.
+VDEV float3 accept_step(const ChaosArgs& A, const float4* pal, const Rng& rng, int fn, float2 pv,
+                        float nz, int dc_hit, float3 dc, float2 p_start, bool past_fuse,
+                        u64* acc_samples, u64* acc_in) {
+  float3 sp = make_float3(pv.x, pv.y, nz);
+#if HAS_FINAL
+  {
+    const float* F = c_xf + FINAL_SLOT * 116;
+    bool apply = true;
+    if (F[10] != 1.0f) apply = rand01(rng) < F[10];
+    if (apply) {
+      Ctx cf;
+      cf.rng = rng;
+      cf.a0 = make_float4(F[0], F[1], F[2], F[3]);
+      cf.a1 = make_float4(F[4], F[5], F[6], F[7]);
+      ChainOut of;
+      of.dc_hit = dc_hit;
+      of.dc = dc;
+      final_chain(pv, nz, cf, of);
+      dc_hit = of.dc_hit;
+      dc = of.dc;
+      if (!bad_point(of.pv)) sp = make_float3(of.pv.x, of.pv.y, of.nz);
+    }
+  }
+#endif
+  const float mag = fmaxf(fmaxf(fabsf(pv.x), fabsf(pv.y)), 1e-30f);
+  const float amp = mag * A.jitter;
+  float jx = (rand01(rng) - 0.5f) * amp;
+  float jy = (rand01(rng) - 0.5f) * amp;
+  if (past_fuse) {
+    *acc_samples += 1;
+    splat(A, pal, sp, p_start, c_xf[fn * 116 + 10], dc_hit, dc, acc_in);
+  }
+  return make_float3(pv.x + jx, pv.y + jy, nz);
+}
+
 // --------------------------------------------------------------- kernel
 extern "C" __global__ void __launch_bounds__(WPB)
 chaos_kernel(const __grid_constant__ ChaosArgs A) {
@@ -460,6 +541,314 @@ chaos_kernel(const __grid_constant__ ChaosArgs A) {
     atomicAdd(&A.counters[1], acc_in);
   }
 }
+
+#if QUEUE
+// ------------------------------------------------------------ queue kernel
+// Compiled beside chaos_kernel for genomes of up to 32 xforms; the host
+// picks one of the two per launch.  One CTA per SM owns QP walker slots.
+// Their records (ISAAC state, point, counters) live in global memory,
+// private to the CTA and small enough to stay in L2; the slot ids wait in
+// one shared-memory ring per xform.  A warp takes up to 32 slots from one
+// ring, stages their records in shared memory, runs one iteration of each
+// -- its lanes execute that xform's chain together -- writes the records
+// back and pushes every slot onto the ring of the xform its walker picked
+// next.  Warps never wait for one another at a barrier.  The warps of a
+// CTA keep to the CTA's current ring while it holds a full batch, so an SM
+// runs one xform's code at a time and the instruction working set stays
+// small however many xforms the genome has; keeping only the ring entries
+// on chip is what lets a CTA hold enough walkers for that.
+//
+// The next pick is drawn at the end of an iteration from the walker's own
+// stream -- the first draw of its next iteration, where the reference
+// draws it.  A finished walker's slot is reseeded with the next walker of
+// the launch (sched[0] counts walkers handed out) or retired.
+//
+// Rings: QP cells of u16 each; a ring never holds more than QP entries
+// because each slot is in at most one ring; head and tail only grow.  A
+// cell is FREE(lap) = lap << 11 or FULL(lap, slot) = 0x8000 | lap << 11 |
+// slot, lap = (position / QP) mod 16.  A producer reserves a position with
+// atomicAdd on tail, waits for FREE(lap) there and writes FULL(lap, slot);
+// a consumer reserves positions with atomicCAS on head, waits for
+// FULL(lap), takes the slot and writes FREE(lap + 1).  The cell a producer
+// waits for was reserved by a consumer one lap earlier (a ring would
+// otherwise hold more than QP slots), so every wait ends; each is bounded
+// all the same, and past the limit the kernel sets sched[1] and returns,
+// which the host reports.
+//
+// Records are only ever touched by their own CTA, so CTA-scope fences order
+// a record's write-back before its slot is pushed, and a slot's take before
+// its record is read; the record traffic bypasses L1 (ld/st .cg).
+#define QP 2048                // walker slots per CTA (slot ids fit 11 bits)
+#define QP_LOG2 11
+#define QFULL 0x8000u
+#define WR_WORDS 48            // record stride in u32 (192 B)
+#define WR_PARTS 11            // uint4 parts that carry data (words 0..43)
+#define SST 33                 // staging stride between ISAAC fields: conflict-free
+#define QSPIN_LIMIT (1u << 22)
+#define QIDLE_CYCLES 4000000000ll  // ~2 s at 1.97 GHz without work while walkers are live
+
+// Bounded wait for cell c to satisfy (v & mask) == want; returns the value
+// seen, or 0xffffffff after QSPIN_LIMIT polls.
+VDEV u32 q_wait(volatile unsigned short* c, u32 mask, u32 want) {
+  for (u32 spins = 0; spins < QSPIN_LIMIT; ++spins) {
+    const u32 v = *c;
+    if ((v & mask) == want) return v;
+  }
+  return 0xffffffffu;
+}
+// Append slot s at ring position pos; false on a timed-out wait.
+VDEV bool q_put(unsigned short* ring_k, u32 pos, u32 s) {
+  volatile unsigned short* c = ring_k + (pos & (QP - 1));
+  const u32 lap = (pos >> QP_LOG2) & 15u;
+  if (q_wait(c, 0xffffu, lap << 11) == 0xffffffffu) return false;
+  *c = (unsigned short)(QFULL | (lap << 11) | s);
+  return true;
+}
+// Take the slot at ring position pos; false on a timed-out wait.
+VDEV bool q_take(unsigned short* ring_k, u32 pos, u32* s) {
+  volatile unsigned short* c = ring_k + (pos & (QP - 1));
+  const u32 lap = (pos >> QP_LOG2) & 15u;
+  const u32 v = q_wait(c, 0xf800u, QFULL | (lap << 11));
+  if (v == 0xffffffffu) return false;
+  *s = v & (QP - 1);
+  *c = (unsigned short)(((lap + 1u) & 15u) << 11);
+  return true;
+}
+VDEV u32 vld(const u32* p) { return *(const volatile u32*)p; }
+
+// Staged walker of lane `lane`: ISAAC fields at sst[k * SST + lane]; record
+// words 36..41 at sf[(w - 36) * 32 + lane]: x, y, z bits, iteration index,
+// fuse + iterations, prev xform (low byte, 0xff = none) | bad count << 8.
+// Seed walker lw of the launch into it (src/isaac.ts:194-229) and draw its
+// start point (chaos.wgsl:8302-8305).
+VDEV void q_seed(const ChaosArgs& A, u32* sst, u32* sf, u32 lane, u64 lw) {
+  const Rng r{sst + lane, SST};
+  seed_walker(r, A.seed, A.walker_base + lw);
+  const float x0 = rand_11(r);
+  const float y0 = rand_11(r);
+  const float z0 = rand01(r);
+  sf[lane] = __float_as_uint(x0);
+  sf[32 + lane] = __float_as_uint(y0);
+  sf[64 + lane] = __float_as_uint(z0);
+  sf[96 + lane] = 0u;
+  sf[128 + lane] = (u32)(A.iters_base + (lw < A.iters_extra ? 1ull : 0ull) + A.fuse);
+  sf[160 + lane] = 0xffu;
+}
+// Record <-> staging for the first n lanes' slots in ssl (coalesced).
+VDEV void q_load(const ChaosArgs& A, const u32* ssl, u32 n, u32 lane, u32* sst, u32* sf) {
+  const u32* base = A.wrec + (u64)blockIdx.x * QP * WR_WORDS;
+  for (u32 q = lane; q < n * WR_PARTS; q += 32u) {
+    const u32 r = q / WR_PARTS, j = q % WR_PARTS;
+    const uint4 v = __ldcg((const uint4*)(base + (u64)ssl[r] * WR_WORDS) + j);
+    const u32 w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const u32 wd = j * 4u + (u32)e;
+      if (wd < 36u) sst[wd * SST + r] = w[e];
+      else if (wd < 42u) sf[(wd - 36u) * 32u + r] = w[e];
+    }
+  }
+}
+VDEV void q_store(const ChaosArgs& A, const u32* ssl, u32 n, u32 lane, const u32* sst,
+                  const u32* sf) {
+  u32* base = A.wrec + (u64)blockIdx.x * QP * WR_WORDS;
+  for (u32 q = lane; q < n * WR_PARTS; q += 32u) {
+    const u32 r = q / WR_PARTS, j = q % WR_PARTS;
+    u32 w[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const u32 wd = j * 4u + (u32)e;
+      w[e] = wd < 36u ? sst[wd * SST + r] : (wd < 42u ? sf[(wd - 36u) * 32u + r] : 0u);
+    }
+    __stcg((uint4*)(base + (u64)ssl[r] * WR_WORDS) + j, make_uint4(w[0], w[1], w[2], w[3]));
+  }
+}
+
+extern "C" __global__ void __launch_bounds__(QWARPS * 32, 1)
+chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float4* pal = (float4*)smem;                                  // [256]
+  u32* stage = (u32*)(pal + 256);                               // [QWARPS][36*SST + 7*32]
+  unsigned short* ring = (unsigned short*)(stage + QWARPS * (36 * SST + 7 * 32));  // [NXF][QP]
+  unsigned short* pst = ring + NXF * QP;                        // pick boundaries
+  u32* qhead = (u32*)(pst + ((MAXRANK * NXF + 1) & ~1));
+  u32* qtail = qhead + NXF;
+  int* live = (int*)(qtail + NXF);
+  u32* aff = (u32*)(live + 1);                                  // the CTA's current ring
+
+  const u32 t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  for (u32 i = t; i < 256u; i += blockDim.x) pal[i] = ((const float4*)A.palette)[i];
+  for (u32 i = t; i < (u32)(MAXRANK * NXF); i += blockDim.x) pst[i] = A.pick_start[i];
+  for (u32 i = t; i < (u32)(NXF * QP); i += blockDim.x) ring[i] = 0;  // FREE(lap 0)
+  if (t < (u32)NXF) { qhead[t] = 0u; qtail[t] = 0u; }
+  if (t == 0) { *live = 0; *aff = 0u; }
+  __syncthreads();
+  u32* sst = stage + warp * (36 * SST + 7 * 32);
+  u32* sf = sst + 36 * SST;
+  u32* ssl = sf + 6 * 32;                                       // slot of each lane
+
+  // ---- fill the slots, 32 at a time per warp
+  for (u32 b = warp * 32u; b < A.cta_slots; b += QWARPS * 32u) {
+    const u32 s = b + lane;
+    bool have = false;
+    u32 fn = 0u;
+    if (s < A.cta_slots) {
+      const u64 lw = atomicAdd((unsigned long long*)&A.sched[0], 1ull);
+      if (lw < A.n_walkers) {
+        q_seed(A, sst, sf, lane, lw);
+        fn = pick_xform(pst, NXF, irand(Rng{sst + lane, SST}) & 16383u);
+        have = true;
+      }
+    }
+    ssl[lane] = s;
+    __syncwarp();
+    // Store every lane whose slot exists (a prefix of the warp); slots that
+    // got no walker are never queued, so their records are never read.
+    const u32 nb = A.cta_slots - b < 32u ? A.cta_slots - b : 32u;
+    q_store(A, ssl, nb, lane, sst, sf);
+    __threadfence_block();
+    __syncwarp();
+    if (have) {
+      const u32 pos = atomicAdd(&qtail[fn], 1u);  // fewer than QP so far: lap 0, cell FREE(0)
+      ring[fn * QP + (pos & (QP - 1))] = (unsigned short)(QFULL | s);
+      atomicAdd(live, 1);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+
+  u64 acc_samples = 0, acc_in = 0;
+  long long idle_since = -1;
+  bool fault = false;
+  while (!fault) {
+    // ---- choose a ring: the CTA's current one while it holds a full batch
+    u32 k = *(volatile u32*)aff;
+    const u32 hk = vld(&qhead[k]);
+    const u32 len = vld(&qtail[k]) - hk;
+    if (len < 32u) {  // else the longest ring (ties: lowest xform)
+      u32 l2 = 0u;
+      if (lane < (u32)NXF) {
+        const u32 hh = vld(&qhead[lane]);  // head first: tail >= head at any later time
+        l2 = vld(&qtail[lane]) - hh;
+      }
+      u32 best = l2, bk = lane;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const u32 ol = __shfl_xor_sync(0xffffffffu, best, o);
+        const u32 ok = __shfl_xor_sync(0xffffffffu, bk, o);
+        if (ol > best || (ol == best && ok < bk)) { best = ol; bk = ok; }
+      }
+      if (best == 0u) {
+        if (*(volatile int*)live == 0) break;
+        const long long now = clock64();
+        if (idle_since < 0) idle_since = now;
+        else if (now - idle_since > QIDLE_CYCLES) { fault = true; break; }
+        __nanosleep(64);
+        continue;
+      }
+      k = bk;
+      if (lane == 0) *(volatile u32*)aff = k;
+    }
+    idle_since = -1;
+    // ---- reserve up to 32 positions of ring k
+    u32 h = 0u, n = 0u;
+    if (lane == 0) {
+      h = vld(&qhead[k]);
+      const u32 avail = vld(&qtail[k]) - h;
+      n = avail < 32u ? avail : 32u;
+      if (n > 0u && atomicCAS(&qhead[k], h, h + n) != h) n = 0u;
+    }
+    n = __shfl_sync(0xffffffffu, n, 0);
+    if (n == 0u) continue;
+    h = __shfl_sync(0xffffffffu, h, 0);
+    // ---- take the slots and stage their records
+    if (lane < n) {
+      u32 s = 0u;
+      if (q_take(ring + k * QP, h + lane, &s)) ssl[lane] = s;
+      else fault = true;
+    }
+    if (__any_sync(0xffffffffu, fault)) { fault = true; break; }
+    __syncwarp();
+    __threadfence_block();
+    q_load(A, ssl, n, lane, sst, sf);
+    __syncwarp();
+
+    // ---- one iteration of each staged walker (the warp runs xform k)
+    bool push = false;
+    u32 nfn = 0u;
+    if (lane < n) {
+      const Rng rng{sst + lane, SST};
+      const float2 p_start = f2(__uint_as_float(sf[lane]), __uint_as_float(sf[32 + lane]));
+      ChainOut o;
+      run_chain(A, pst, (int)k, p_start, __uint_as_float(sf[64 + lane]), rng, o);
+      float2 pv = o.pv;
+      const float nz = o.nz;
+      u32 i = sf[96 + lane];
+      const u32 pb = sf[160 + lane];
+      u32 consec = pb >> 8;
+      int prev = (int)(pb & 0xffu);
+      if (prev == 0xff) prev = -1;
+      if (bad_point(pv)) {
+        const float bx = rand_11(rng);
+        const float by = rand_11(rng);
+        pv = f2(bx, by);
+        consec += 1u;
+      } else {
+        consec = 0u;
+      }
+      float3 np = make_float3(pv.x, pv.y, nz);
+      if (consec > 0u && consec < 5u) {
+        if (i == 0u) i = 1u;  // the reference's rollback stops at 0
+      } else {
+        if (consec >= 5u) consec = 0u;
+        prev = (int)k;
+        np = accept_step(A, pal, rng, (int)k, pv, nz, o.dc_hit, o.dc, p_start, i >= A.fuse,
+                         &acc_samples, &acc_in);
+        i += 1u;
+      }
+      sf[lane] = __float_as_uint(np.x);
+      sf[32 + lane] = __float_as_uint(np.y);
+      sf[64 + lane] = __float_as_uint(np.z);
+      sf[96 + lane] = i;
+      sf[160 + lane] = ((u32)prev & 0xffu) | (consec << 8);
+      push = true;
+      if (i >= sf[128 + lane]) {  // finished: the next walker of the launch, or retire the slot
+        const u64 lw = atomicAdd((unsigned long long*)&A.sched[0], 1ull);
+        if (lw < A.n_walkers) {
+          q_seed(A, sst, sf, lane, lw);
+          prev = -1;
+        } else {
+          atomicSub(live, 1);
+          push = false;
+        }
+      }
+      if (push) nfn = pick_xform(pst, prev >= 0 ? (u32)prev : (u32)NXF, irand(rng) & 16383u);
+    }
+    __syncwarp();
+    // ---- write the records back, then push the slots
+    q_store(A, ssl, n, lane, sst, sf);
+    __threadfence_block();
+    __syncwarp();
+    const u32 pm = __ballot_sync(0xffffffffu, push);
+    if (push) {
+      const u32 peers = __match_any_sync(pm, nfn);
+      const u32 leader = (u32)(__ffs(peers) - 1);
+      u32 base = 0u;
+      if (lane == leader) base = atomicAdd(&qtail[nfn], (u32)__popc(peers));
+      base = __shfl_sync(peers, base, leader);
+      const u32 rank = (u32)__popc(peers & ((1u << lane) - 1u));
+      if (!q_put(ring + nfn * QP, base + rank, ssl[lane])) fault = true;
+    }
+    fault = __any_sync(0xffffffffu, fault);
+    __syncwarp();
+  }
+  if (fault && lane == 0) atomicOr((unsigned long long*)&A.sched[1], 1ull);
+  if (A.counters) {
+    atomicAdd(&A.counters[0], acc_samples);
+    atomicAdd(&A.counters[1], acc_in);
+  }
+}
+#endif  // QUEUE
 
 // ------------------------------------------------------- stage test kernels
 // Xform pick of an explicit draw stream (chaos.wgsl:8343-8348).

@@ -116,8 +116,9 @@ class Renderer:
                 walker_jitter: float = DEFAULT_WALKER_JITTER, color_mode: str = "palette",
                 flow_strength: float = 1.0, flow_scale: float = DEFAULT_FLOW_SCALE, trap=None,
                 phase_strength: float = 1.0, phase_freq: float = 1.0, exact_walkers: bool = False,
-                aggregate: bool = False) -> None:
-        """Accumulate walkers x iters samples (src/renderer.ts:227)."""
+                aggregate: bool = False, kernel: str = "auto") -> None:
+        """Accumulate walkers x iters samples (src/renderer.ts:227).
+        kernel: "auto" (the autotuner's choice), "barrier" or "queue"."""
         gg = genome if isinstance(genome, GpuGenome) else GpuGenome(genome)
         trap = trap or {}
         modes = {"palette": 0, "flow": 1, "trap-distance": 2, "phase": 3}
@@ -128,7 +129,8 @@ class Renderer:
             1 if trap.get("mode") == "rings" else 0, trap.get("cx", 0.0), trap.get("cy", 0.0),
             trap.get("radius", 0.5), trap.get("angle", 0.0), trap.get("falloff", 2.0),
             trap.get("freq", 4.0), trap.get("strength", 1.0), phase_strength, phase_freq,
-            (_lib.ITER_EXACT_WALKERS if exact_walkers else 0) | (_lib.ITER_AGGREGATE if aggregate else 0))
+            (_lib.ITER_EXACT_WALKERS if exact_walkers else 0) | (_lib.ITER_AGGREGATE if aggregate else 0)
+            | {"auto": 0, "barrier": _lib.ITER_KERNEL_BARRIER, "queue": _lib.ITER_KERNEL_QUEUE}[kernel])
         _lib.check(_lib.lib().pyr3_iterate(self._h, C.byref(gg.c), C.byref(o)))
 
     def present_opts(self, genome: Genome, force_de_off: bool = False,

@@ -202,6 +202,31 @@ def test_variations_match_flam3_goldens():
 def _c1_histogram(W, H, iters=3000, walkers=1024, seed=5):
     g = workloads.plain_small()
     g.scale = W / 4
+    return _ref_histogram(g, W, H, iters, walkers, seed)
+
+
+def _wide_genome(n=40, seed=5):
+    """n xforms of {linear, sinusoidal, spherical} (the C1 recipe), more than
+    the queue kernel takes, so the barrier-synchronised kernel runs."""
+    import copy
+
+    rng = np.random.default_rng(seed)
+    g = workloads.plain_small()
+    base = g.xforms
+    xs = []
+    for k in range(n):
+        x = copy.deepcopy(base[k % len(base)])
+        x.a, x.b, x.c, x.d, x.e, x.f = (float(v) for v in rng.uniform(-1.0, 1.0, 6))
+        x.weight = float(rng.uniform(0.2, 1.0))
+        x.color = float(rng.uniform(0.0, 1.0))
+        xs.append(x)
+    g.xforms = xs
+    return g
+
+
+def _ref_histogram(g, W, H, iters, walkers, seed):
+    """The reference's chaos_main (translated WGSL, CPU) over `walkers`
+    ISAAC streams of `iters` post-fuse iterations."""
     xf = G.pack_xforms(g)
     pal = G.bake_lut(g.palette)
     distrib = O.pack_xform_distrib([x.weight for x in g.xforms])
@@ -250,20 +275,28 @@ def _collapse(hist, W, H, os_):
     return h.reshape(H, os_, W, os_, 4).sum(axis=(1, 3))
 
 
-def test_whole_render_statistical_parity():
-    """C1 genome on a 160x120 canvas (~2500 samples per pixel): the CUDA
-    renderer (its own walker pool) vs the reference's chaos_main on the CPU
-    (1024 walkers), equal sample count.  Trajectories diverge chaotically, so
-    the comparison is statistical: log-density relative L1 <= 1% (and within
-    1.5x of the reference-vs-reference noise floor at another seed) and
-    tonemapped PSNR >= 40 dB."""
+@pytest.mark.parametrize("kind", ["c1_queue_kernel", "c1_barrier_kernel", "wide_barrier_kernel"])
+def test_whole_render_statistical_parity(kind):
+    """A genome on a 160x120 canvas: the CUDA renderer (its own walker pool)
+    vs the reference's chaos_main on the CPU (1024 walkers), equal sample
+    count.  Trajectories diverge chaotically, so the comparison is
+    statistical: log-density relative L1 <= 1% (or within 1.5x of the
+    reference-vs-reference noise floor at another seed) and tonemapped PSNR
+    >= 40 dB.  The C1 genome (3 xforms) runs on each chaos kernel; the
+    40-xform genome has only the barrier-synchronised one."""
     W, H = 160, 120
-    walkers, iters = 1024, 48_000
-    g, pal, ref_hist, samples = _c1_histogram(W, H, iters=iters, walkers=walkers, seed=9)
-    _, _, ref2_hist, _ = _c1_histogram(W, H, iters=iters, walkers=walkers, seed=31)
+    # The 40-xform attractor covers more of the canvas: 6.7x the samples
+    # bring its noise floor well inside the bars.
+    wide = kind == "wide_barrier_kernel"
+    walkers, iters = 1024, (320_000 if wide else 48_000)
+    g = _wide_genome() if wide else workloads.plain_small()
+    g.scale = W / 4
+    g, pal, ref_hist, samples = _ref_histogram(g, W, H, iters, walkers, 9)
+    _, _, ref2_hist, _ = _ref_histogram(g, W, H, iters, walkers, 31)
     r = R.create_renderer(W, H, 1)
     r.reset(g)
-    r.iterate(g, seed=77, walkers=walkers, iters_per_walker=iters)
+    r.iterate(g, seed=77, walkers=walkers, iters_per_walker=iters,
+              kernel="queue" if kind == "c1_queue_kernel" else "barrier")
     s, _ = r.counters()
     assert s == samples
     dev_hist, _, _ = r.read_histogram()
@@ -284,4 +317,45 @@ def test_whole_render_statistical_parity():
     psnr = 10 * np.log10(1.0 / max(mse, 1e-20))
     print(f"log-density L1 {l1:.4%} (ref-vs-ref {floor:.4%})  PSNR {psnr:.2f} dB")
     assert psnr >= 40.0
+    r.destroy()
+
+
+def test_queue_kernel_refills_walker_slots():
+    """More walkers than the resident slots (exact-walkers mode), so slots
+    are refilled as walkers finish: every walker runs exactly its
+    iterations, the count channel holds 255 per in-canvas splat, and the
+    kernel reports no scheduling fault."""
+    g = workloads.plain_small()
+    g.scale = 320 / 4
+    r = R.create_renderer(320, 240, 1)
+    r.reset(g)
+    walkers, iters = 400_000, 40
+    r.iterate(g, seed=3, walkers=walkers, iters_per_walker=iters, exact_walkers=True,
+              kernel="queue")
+    r.sync()
+    s, n_in = r.counters()
+    assert s == walkers * iters
+    hist, _, _ = r.read_histogram()
+    assert int(hist.reshape(-1, 4)[:, 3].astype(np.uint64).sum()) == 255 * n_in
+    assert n_in > 0
+    r.destroy()
+
+
+def test_kernel_autotuner_splits_the_first_large_launch():
+    """The first launch of >= 2^26 samples of a structure runs trials on
+    both chaos kernels and the rest on the faster: the sample count is
+    exact, the in-canvas splats match the count channel, and a second
+    launch (the remembered choice) still counts exactly."""
+    g = workloads.plain_small()
+    g.xforms[0].variations.append(G.Variation(G.variation_index("swirl"), 0.05))  # a fresh structure
+    g.scale = 320 / 4
+    r = R.create_renderer(320, 240, 1)
+    r.reset(g)
+    total = 70_000_000
+    r.iterate(g, seed=5, walkers=1000, iters_per_walker=total // 1000)
+    r.iterate(g, seed=6, walkers=1000, iters_per_walker=total // 1000)
+    s, n_in = r.counters()
+    assert s == 2 * (total // 1000) * 1000
+    hist, _, _ = r.read_histogram()
+    assert int(hist.reshape(-1, 4)[:, 3].astype(np.uint64).sum()) == 255 * n_in
     r.destroy()
