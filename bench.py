@@ -261,10 +261,16 @@ def bench_ours(args, ws, rank, local, dist):
     e2e = ws * samples * args.steps / (e2e_max / 1e3)
     peak, peak_kind = _peaks()
     # Dominant kernel: the chaos kernel.  Algorithmic bytes per launch: every
-    # in-canvas splat reads and writes one 16-byte RGBA u32 bucket.
-    splats_per_launch = n_splats / max(1, (args.steps + args.warmup + max(1, args.warmup // 2)))
+    # in-canvas splat reads and writes one 16-byte RGBA u32 bucket.  The
+    # counters restart at every reset, so they hold the last timed step.
+    splats_per_launch = n_splats
     mean_chaos = statistics.mean(chaos_ms)
     achieved = splats_per_launch * 32.0 / (mean_chaos / 1e3) / 1e9
+    traffic = None  # DRAM bytes per launch measured by ncu for this workload at full size
+    tpath = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "roofline_traffic.json")
+    if not args.samples and os.path.exists(tpath):
+        t = json.load(open(tpath)).get(args.config)
+        traffic = t["dram_bytes_per_launch"] if t else None
     h2d = 4096 + gg.xforms.nbytes + (len(g.xforms) + 1) * len(g.xforms) * 2
     line = {
         "metric": CONFIGS[args.config][0], "value": value, "unit": "iters/s", "n_gpus": ws,
@@ -281,9 +287,10 @@ def bench_ours(args, ws, rank, local, dist):
                 "d2h_bytes_per_step": int(host_img.nbytes)},
         "chaos_kernel_ms": mean_chaos,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": traffic,
                      "note": f"chaos kernel; algorithmic bytes = 32 B (16 B bucket read+write) per "
-                             f"in-canvas splat; peak {peak_kind}"},
+                             f"in-canvas splat ({splats_per_launch} splats per launch); peak {peak_kind}; "
+                             f"the kernel is bound by instruction issue and latency (ncu), not by HBM"},
         "gpu_launches": args.steps * (2 + (1 if g.density is not None else 0)),
         "clocks": clk,
     }
