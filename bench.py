@@ -93,12 +93,13 @@ class Clocks:
 
 
 def _workload(name):
+    """(genome, genome at shutter close or None)."""
     from pyr3_b200 import workloads
 
     g = getattr(workloads, CONFIGS[name][1])()
-    if isinstance(g, tuple):  # motion blur: shutter-open keyframe drives the bench
-        g = g[0]
-    return g
+    if isinstance(g, tuple):  # motion blur: keyframes at shutter open and close
+        return g
+    return g, None
 
 
 def _dist():
@@ -186,7 +187,9 @@ def cpu_reference_rate(g, target_seconds: float = 12.0, threads: int | None = No
 def bench_ours(args, ws, rank, local, dist):
     from pyr3_b200 import _lib, renderer as R
 
-    g = _workload(args.config)
+    from pyr3_b200 import animate
+
+    g, g_close = _workload(args.config)
     W, H = g.size
     os_ = g.oversample
     walkers, iters, samples = R.compute_dispatch(g.quality, W, H)
@@ -210,8 +213,15 @@ def bench_ours(args, ws, rank, local, dist):
     L2_FLUSH = 256 << 20
 
     def step_device(seed):
-        _lib.check(lib.pyr3_reset(h, _lib.ptr(pal)))
-        r.iterate(gg, seed, walkers, iters)
+        if g_close is None:
+            _lib.check(lib.pyr3_reset(h, _lib.ptr(pal)))
+            _lib.check(lib.pyr3_mark(h, 4))
+            r.iterate(gg, seed, walkers, iters)
+        else:  # one motion-blurred frame: 8 sub-frames into one histogram
+            _lib.check(lib.pyr3_mark(h, 4))
+            n, _ = animate.render_motion_frame(r, g, g_close, 0.5, ntemporal=8, seed=seed)
+            assert n == samples
+        _lib.check(lib.pyr3_mark(h, 5))
         _lib.check(lib.pyr3_present_device(h, C.byref(p), samples, C.c_void_p(out_dev.data_ptr()),
                                            _lib.OUT_RGBA8))
 
@@ -229,7 +239,8 @@ def bench_ours(args, ws, rank, local, dist):
         ms = C.c_float()
         _lib.check(lib.pyr3_elapsed(h, 0, 1, C.byref(ms)))
         total_ms += ms.value
-        chaos_ms.append(r.last_iterate_ms())
+        _lib.check(lib.pyr3_elapsed(h, 4, 5, C.byref(ms)))
+        chaos_ms.append(ms.value)
     clk = clocks.stop() if clocks else None
     n_samples, n_splats = r.counters()
     _barrier(dist)
@@ -237,17 +248,21 @@ def bench_ours(args, ws, rank, local, dist):
 
     # e2e through the public API: host palette + genome in, RGBA8 image out
     host_img = np.zeros((H, W, 4), np.uint8)
-    for k in range(max(1, args.warmup // 2)):
-        r.reset(g)
-        r.iterate(g, 5000 + k, walkers, iters)
+    def step_public(seed):
+        if g_close is None:
+            r.reset(g)
+            r.iterate(g, seed, walkers, iters)
+        else:
+            animate.render_motion_frame(r, g, g_close, 0.5, ntemporal=8, seed=seed)
         r.present(g, samples, out=host_img)
+
+    for k in range(max(1, args.warmup // 2)):
+        step_public(5000 + k)
     e2e_ms = 0.0
     for k in range(args.steps):
         _lib.check(lib.pyr3_flush_l2(h, L2_FLUSH))
         _lib.check(lib.pyr3_mark(h, 2))
-        r.reset(g)
-        r.iterate(g, 7000 + k, walkers, iters)
-        r.present(g, samples, out=host_img)
+        step_public(7000 + k)
         _lib.check(lib.pyr3_mark(h, 3))
         ms = C.c_float()
         _lib.check(lib.pyr3_elapsed(h, 2, 3, C.byref(ms)))
@@ -281,6 +296,7 @@ def bench_ours(args, ws, rank, local, dist):
                    "quality_spp": g.quality, "samples_per_step": samples,
                    "xforms": len(g.xforms), "final_xform": g.finalxform is not None,
                    "density_estimation": g.density is not None,
+                   "temporal_samples": 8 if g_close is not None else 1,
                    "l2": "256 MiB scratch overwritten between timed steps",
                    "parallelism": f"replicas x{ws}"},
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": int(h2d),
@@ -291,7 +307,8 @@ def bench_ours(args, ws, rank, local, dist):
                      "note": f"chaos kernel; algorithmic bytes = 32 B (16 B bucket read+write) per "
                              f"in-canvas splat ({splats_per_launch} splats per launch); peak {peak_kind}; "
                              f"the kernel is bound by instruction issue and latency (ncu), not by HBM"},
-        "gpu_launches": args.steps * (2 + (1 if g.density is not None else 0)),
+        "gpu_launches": args.steps * ((8 if g_close is not None else 1) + 1 +
+                                      (1 if g.density is not None else 0)),
         "clocks": clk,
     }
     if ws == 1 and not args.no_cpu_baseline:
@@ -305,7 +322,7 @@ def bench_ours(args, ws, rank, local, dist):
 def bench_reference(args, ws, rank, local, dist):
     if rank != 0:
         return None
-    g = _workload(args.config)
+    g, _ = _workload(args.config)
     per = max(2.0, 60.0 / max(1, args.steps + args.warmup))
     for _ in range(args.warmup):
         cpu_reference_rate(g, target_seconds=per)

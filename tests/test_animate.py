@@ -1,0 +1,122 @@
+"""Motion-blurred frames (src/temporal-filter.ts, src/animate-render.ts,
+src/interpolate.ts): CPU checks restating the reference's own test cases
+(src/temporal-filter.test.ts, src/animate-render.test.ts), and a GPU check of
+a whole motion-blurred frame against the reference's chaos loop run per
+sub-frame."""
+import copy
+
+import numpy as np
+import pytest
+
+from pyr3_b200 import animate as A
+from pyr3_b200 import workloads
+
+
+def test_temporal_filter_matches_reference_cases():
+    assert A.temporal_filter(1, "box", 1.0, 0) == ([0.0], [1.0], 1.0)
+    d, f, s = A.temporal_filter(4, "box", 1.0, 0)
+    assert d[0] == pytest.approx(-0.5) and d[3] == pytest.approx(0.5)
+    assert d[1] - d[0] == pytest.approx(1 / 3)
+    assert f == [1, 1, 1, 1] and s == pytest.approx(1.0)
+    d, _, _ = A.temporal_filter(4, "box", 2.0, 0)
+    assert d[0] == pytest.approx(-1) and d[3] == pytest.approx(1)
+    _, f, s = A.temporal_filter(11, "gaussian", 1.0, 0)
+    assert f[5] > f[0] and max(f) == pytest.approx(1.0) and 0 < s < 1
+    _, f, _ = A.temporal_filter(10, "exp", 1.0, 2.0)
+    assert f[9] == pytest.approx(1.0) and f[0] < f[9]
+    _, f, _ = A.temporal_filter(10, "exp", 1.0, -2.0)
+    assert f[0] == pytest.approx(1.0) and f[9] < f[0]
+    _, f, _ = A.temporal_filter(10, "exp", 1.0, 0.0)
+    assert all(v == pytest.approx(1.0) for v in f)
+
+
+def test_apportion_walkers_matches_reference_cases():
+    out = A.apportion_walkers(1024, [1] * 2000)
+    assert sum(out) == 1024 and sum(1 for w in out if w == 0) > 900
+    out = A.apportion_walkers(100, [0.05, 0.3, 1.0, 0.3, 0.05])
+    assert sum(out) == 100 and out[2] > out[1] and out[2] > out[3]
+    assert A.apportion_walkers(64, [0, 0, 1, 0]) == [0, 0, 64, 0]
+    assert A.apportion_walkers(0, [1, 1, 1]) == [0, 0, 0]
+    assert A.apportion_walkers(100, [0, 0]) == [0, 0]
+    assert A.apportion_walkers(100, []) == []
+    for n in (3, 7, 1000, 4096):
+        out = A.apportion_walkers(1024, [1] * n)
+        assert sum(out) == 1024 and min(out) >= 0
+
+
+def test_interpolate_linear_endpoints_and_midpoint():
+    g0, g1 = workloads.motion_4k()
+    a = A.interpolate_linear(g0, g1, 0.0)
+    b = A.interpolate_linear(g0, g1, 1.0)
+    m = A.interpolate_linear(g0, g1, 0.5)
+    for x, x0, x1, xa, xb in zip(m.xforms, g0.xforms, g1.xforms, a.xforms, b.xforms):
+        for k in "abcdef":
+            assert getattr(xa, k) == pytest.approx(getattr(x0, k))
+            assert getattr(xb, k) == pytest.approx(getattr(x1, k))
+            assert getattr(x, k) == pytest.approx(0.5 * getattr(x0, k) + 0.5 * getattr(x1, k))
+    bad = copy.deepcopy(g1)
+    bad.xforms = bad.xforms[:-1]
+    with pytest.raises(ValueError):
+        A.interpolate_linear(g0, bad, 0.5)
+
+
+def _motion_pair():
+    """The C1 genome at shutter open and a copy with its affines moved."""
+    g0 = workloads.plain_small()
+    g1 = copy.deepcopy(g0)
+    rng = np.random.default_rng(4)
+    for x in g1.xforms:
+        x.a, x.b, x.c, x.d, x.e, x.f = (v + float(dv) for v, dv in
+                                        zip((x.a, x.b, x.c, x.d, x.e, x.f), rng.uniform(-0.08, 0.08, 6)))
+    return g0, g1
+
+
+@pytest.mark.gpu
+def test_motion_frame_matches_reference_subframe_loop():
+    """4 box-filtered sub-frames of a moving C1 genome on 160x120: the CUDA
+    path (render_motion_frame) vs the reference's chaos_main (translated
+    WGSL, CPU) run for each sub-frame genome with the same walker split into
+    one histogram, at equal samples: log-density L1 within 1% or 1.5x the
+    reference-vs-reference floor."""
+    from oracle import oracle as O
+    from pyr3_b200 import genome as G, renderer as R
+
+    W, H, iters = 160, 120, 48_000
+    g0, g1 = _motion_pair()
+    for g in (g0, g1):
+        g.scale = W / 4
+        g.quality = 1024 * iters / (W * H)
+
+    def ref(seed):
+        hist = np.zeros(W * H * 4, np.uint32)
+        deltas, filt, _ = A.temporal_filter(4)
+        counts = A.apportion_walkers(1024, filt)
+        for i, w in enumerate(counts):
+            sub = A.interpolate_linear(g0, g1, 0.5 + deltas[i])
+            u = np.zeros(31, np.uint32)
+            f, i32 = u.view(np.float32), u.view(np.int32)
+            u[0], u[1], u[2], u[3] = W, H, iters, 200
+            f[4], f[5], f[6] = sub.scale, 0.0, 0.0
+            u[7] = (seed + i * A.GOLDEN) & 0xFFFFFFFF
+            i32[8] = -1
+            u[12] = w
+            f[13] = 1e-7
+            O.ref_chaos_run(u, G.pack_xforms(sub), len(sub.xforms), G.bake_lut(sub.palette),
+                            O.pack_xform_distrib([x.weight for x in sub.xforms]),
+                            O.pack_isaac_states(w, u[7]), 0, w, hist, 16)
+        return hist
+
+    def logd(h):
+        return np.log1p(h.reshape(-1, 4)[:, 3].astype(np.float64) / 255.0)
+
+    r = R.create_renderer(W, H, 1)
+    samples, counts = A.render_motion_frame(r, g0, g1, 0.5, ntemporal=4, seed=77)
+    assert sum(counts) == 1024 and samples == 1024 * iters
+    assert r.counters()[0] == samples
+    dev, _, _ = r.read_histogram()
+    a, b, b2 = logd(dev), logd(ref(9)), logd(ref(31))
+    l1 = float(np.abs(a - b).sum() / b.sum())
+    floor = float(np.abs(b2 - b).sum() / b.sum())
+    print(f"motion log-density L1 {l1:.4%} (ref-vs-ref {floor:.4%})")
+    assert l1 <= max(0.01, 1.5 * floor), (l1, floor)
+    r.destroy()
