@@ -99,6 +99,16 @@ typedef struct {
   float background[3];
   int32_t transparent;
   double scale;             /* genome.scale (calibration k2) */
+  /* Colour curves (src/channel-curves.ts, visualize_u32.wgsl:217-231):
+   * bit mask composite 1, r 2, g 4, b 8, luma 16 (0 = off) and the baked
+   * 5 x 256 f32 LUT in host memory (read only when the mask is non-zero). */
+  uint32_t curves_active;
+  const float *curves;
+  /* HSL adjustment (visualize_u32.wgsl:234-243; src/visualize.ts:194-198):
+   * hue offset in degrees, saturation multiplier and lightness addend
+   * (the genome's percentages / 100). */
+  int32_t hsl_active;
+  float hsl_hue, hsl_sat, hsl_light;
 } pyr3_present_opts;
 
 #define PYR3_OUT_RGBA8 0      /* W x H x 4 u8 (rgba8unorm) */
@@ -134,6 +144,10 @@ int pyr3_present_device(pyr3_renderer *r, const pyr3_present_opts *p, uint64_t t
 /* Renderer.readHistogram (src/renderer.ts:209, src/chaos.ts:293): raw
  * super-res histogram, superW*superH*4 u32 (R, G, B, count). */
 int pyr3_read_histogram(pyr3_renderer *r, uint32_t *host_out);
+/* histogramToLinearRgba (src/export-linear.ts:24-47) of the current
+ * histogram, computed on the device: width x height x RGBA f32 linear,
+ * scene-referred values (k1, k2 from deriveCalibration, src/calibration.ts). */
+int pyr3_read_linear(pyr3_renderer *r, double k1, double k2, float *host_out);
 /* Renderer.readIndexMap (src/renderer.ts:205): superW*superH u32 colour
  * index sums (valid after iterating with capture on). */
 int pyr3_read_index_map(pyr3_renderer *r, uint32_t *host_out);

@@ -443,7 +443,20 @@ typedef struct {
     float k1, k2, gamma, vibrancy, highpow, linrange;
     float bg[3];
     int transparent;
+    unsigned curves_active;   /* composite 1, r 2, g 4, b 8, luma 16 */
+    const float *curves;      /* 5 x 256 */
+    int hsl_active;
+    float hsl_hue, hsl_sat, hsl_light;
 } or_viz;
+
+/* visualize_u32.wgsl:51-56 (lut). */
+static float or_curve_lut(const float *lut, int ch, float x) {
+    float idx = fminf(fmaxf(x, 0.0f), 1.0f) * 255.0f;
+    unsigned i0 = (unsigned)floorf(idx);
+    unsigned i1 = i0 + 1u < 255u ? i0 + 1u : 255u;
+    float t = idx - (float)i0;
+    return lut[ch * 256 + i0] * (1.0f - t) + lut[ch * 256 + i1] * t;
+}
 
 /* visualize_u32.wgsl:53-72 (rgb2hsv). */
 static void or_rgb2hsv(const float c[3], float o[3]) {
@@ -576,6 +589,28 @@ OR_EXPORT void or_visualize(const or_viz *u, const float *kernel1d, const uint32
                 float v = comp / 256.0f;
                 o[c] = fminf(fmaxf(v, 0.0f), 1.0f);
             }
+            if (u->curves_active && u->curves) {  /* visualize_u32.wgsl:217-231 */
+                if (u->curves_active & 16u) {
+                    float l = o[0] * 0.299f + o[1] * 0.587f + o[2] * 0.114f;
+                    float ln = or_curve_lut(u->curves, 4, l);
+                    if (l > 0.0f) { float k = ln / l; o[0] *= k; o[1] *= k; o[2] *= k; }
+                }
+                if (u->curves_active & 2u) o[0] = or_curve_lut(u->curves, 1, o[0]);
+                if (u->curves_active & 4u) o[1] = or_curve_lut(u->curves, 2, o[1]);
+                if (u->curves_active & 8u) o[2] = or_curve_lut(u->curves, 3, o[2]);
+                if (u->curves_active & 1u)
+                    for (int c = 0; c < 3; ++c) o[c] = or_curve_lut(u->curves, 0, o[c]);
+            }
+            if (u->hsl_active) {  /* visualize_u32.wgsl:234-243 */
+                float hsv[3];
+                or_rgb2hsv(o, hsv);
+                hsv[0] = hsv[0] + u->hsl_hue;
+                hsv[0] = hsv[0] - 360.0f * floorf(hsv[0] / 360.0f);
+                hsv[1] = fminf(fmaxf(hsv[1] * u->hsl_sat, 0.0f), 1.0f);
+                hsv[2] = fminf(fmaxf(hsv[2] + u->hsl_light, 0.0f), 1.0f);
+                or_hsv2rgb(hsv, o);
+            }
+            for (int c = 0; c < 3; ++c) o[c] = fminf(fmaxf(o[c], 0.0f), 1.0f);
             o[3] = u->transparent ? alpha : 1.0f;
         }
     }

@@ -97,7 +97,8 @@ def ref():
         R.ref_visualize.argtypes = [C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float,
                                     C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32,
                                     _f32p, C.c_uint32, _f32p, C.c_void_p, C.c_void_p, _f32p,
-                                    C.c_int]
+                                    C.c_int, C.c_uint32, C.c_void_p, C.c_uint32, C.c_float,
+                                    C.c_float, C.c_float]
         _ref = R
     return _ref
 
@@ -197,13 +198,20 @@ class _Viz(C.Structure):
     _fields_ = [("width", C.c_int), ("height", C.c_int), ("oversample", C.c_int),
                 ("fwidth", C.c_int), ("k1", C.c_float), ("k2", C.c_float),
                 ("gamma", C.c_float), ("vibrancy", C.c_float), ("highpow", C.c_float),
-                ("linrange", C.c_float), ("bg", C.c_float * 3), ("transparent", C.c_int)]
+                ("linrange", C.c_float), ("bg", C.c_float * 3), ("transparent", C.c_int),
+                ("curves_active", C.c_uint), ("curves", C.c_void_p), ("hsl_active", C.c_int),
+                ("hsl_hue", C.c_float), ("hsl_sat", C.c_float), ("hsl_light", C.c_float)]
 
 
 def visualize(width, height, oversample, kernel, k1, k2, gamma, vibrancy, highpow, linrange,
-              bg=(0, 0, 0), transparent=False, src_u32=None, src_f32=None):
+              bg=(0, 0, 0), transparent=False, src_u32=None, src_f32=None, curves_active=0,
+              curves=None, hsl=None):
+    """hsl = (hue degrees, sat multiplier, light addend) or None."""
+    cv = np.ascontiguousarray(curves, np.float32) if curves is not None else None
     v = _Viz(width, height, oversample, len(kernel), k1, k2, gamma, vibrancy, highpow, linrange,
-             (C.c_float * 3)(*bg), int(transparent))
+             (C.c_float * 3)(*bg), int(transparent), int(curves_active),
+             cv.ctypes.data if cv is not None else None, 1 if hsl else 0,
+             *(hsl if hsl else (0.0, 1.0, 0.0)))
     out = np.zeros(width * height * 4, np.float32)
     su = np.ascontiguousarray(src_u32, np.uint32) if src_u32 is not None else None
     sf = np.ascontiguousarray(src_f32, np.float32) if src_f32 is not None else None
@@ -254,13 +262,18 @@ def ref_density(hist, width, height, max_rad, min_rad, curve, k1, k2, threads=8)
 
 
 def ref_visualize(width, height, oversample, kernel, k1, k2, gamma, vibrancy, highpow, linrange,
-                  bg=(0, 0, 0), transparent=False, src_u32=None, src_f32=None, threads=8):
+                  bg=(0, 0, 0), transparent=False, src_u32=None, src_f32=None, threads=8,
+                  curves_active=0, curves=None, hsl=None):
     out = np.zeros(width * height * 4, np.float32)
     su = np.ascontiguousarray(src_u32, np.uint32) if src_u32 is not None else None
     sf = np.ascontiguousarray(src_f32, np.float32) if src_f32 is not None else None
+    cv = np.ascontiguousarray(curves, np.float32) if curves is not None else None
+    h = hsl if hsl else (0.0, 1.0, 0.0)
     ref().ref_visualize(width, height, k1, k2, gamma, vibrancy, highpow, linrange, oversample,
                         len(kernel), np.ascontiguousarray(bg, np.float32), int(transparent),
                         np.ascontiguousarray(kernel, np.float32),
                         su.ctypes.data if su is not None else None,
-                        sf.ctypes.data if sf is not None else None, out, threads)
+                        sf.ctypes.data if sf is not None else None, out, threads,
+                        int(curves_active), cv.ctypes.data if cv is not None else None,
+                        1 if hsl else 0, h[0], h[1], h[2])
     return out

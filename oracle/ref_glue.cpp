@@ -157,9 +157,12 @@ REF_EXPORT void ref_visualize(uint32_t width, uint32_t height, float k1, float k
                               float vibrancy, float highpow, float linrange, uint32_t oversample,
                               uint32_t fwidth, const float *bg3, uint32_t transparent,
                               const float *kernel1d, const uint32_t *src_u32,
-                              const float *src_f32, float *out, int threads) {
+                              const float *src_f32, float *out, int threads,
+                              uint32_t curves_active, const float *curves5x256,
+                              uint32_t hsl_active, float hsl_hue, float hsl_sat, float hsl_light) {
   if (threads < 1) threads = 1;
   std::vector<float> curves(5 * 256, 0.0f);
+  if (curves5x256) curves.assign(curves5x256, curves5x256 + 5 * 256);
   std::vector<std::thread> pool;
   for (int t = 0; t < threads; ++t) {
     pool.emplace_back([&, t]() {
@@ -175,8 +178,11 @@ REF_EXPORT void ref_visualize(uint32_t width, uint32_t height, float k1, float k
   NS::u.oversample = oversample;                                        \
   NS::u.fwidth = fwidth;                                                \
   NS::u.background = vec4f(bg3[0], bg3[1], bg3[2], 0.0f);               \
-  NS::u.curvesActive = 0u;                                              \
-  NS::u.hslActive = 0u;                                                 \
+  NS::u.curvesActive = curves_active;                                   \
+  NS::u.hslActive = hsl_active;                                         \
+  NS::u.hslHue = hsl_hue;                                               \
+  NS::u.hslSat = hsl_sat;                                               \
+  NS::u.hslLight = hsl_light;                                           \
   NS::u.transparent = transparent;                                      \
   NS::kernel1d = const_cast<float *>(kernel1d);                         \
   NS::curves = curves.data();

@@ -61,7 +61,9 @@ class PresentOpts(C.Structure):
     _fields_ = [("gamma", C.c_float), ("vibrancy", C.c_float), ("highpow", C.c_float),
                 ("brightness", C.c_float), ("linrange", C.c_float), ("density_on", C.c_int32),
                 ("de_max_rad", C.c_float), ("de_min_rad", C.c_float), ("de_curve", C.c_float),
-                ("background", C.c_float * 3), ("transparent", C.c_int32), ("scale", C.c_double)]
+                ("background", C.c_float * 3), ("transparent", C.c_int32), ("scale", C.c_double),
+                ("curves_active", C.c_uint32), ("curves", C.c_void_p), ("hsl_active", C.c_int32),
+                ("hsl_hue", C.c_float), ("hsl_sat", C.c_float), ("hsl_light", C.c_float)]
 
 
 # name -> (restype, argtypes)
@@ -102,6 +104,7 @@ _SIGS = {
                                                C.c_float, C.POINTER(PresentOpts), C.c_uint64,
                                                C.c_void_p, C.c_int32, C.c_void_p]),
     "pyr3_prepare": (C.c_int, [C.c_void_p, C.POINTER(GenomeC)]),
+    "pyr3_read_linear": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p]),
     "pyr3_jit_compile": (C.c_int, [C.POINTER(GenomeC), C.c_int32, C.POINTER(C.c_uint64)]),
     "pyr3_jit_source": (C.c_int, [C.POINTER(GenomeC), C.c_char_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     "pyr3_jit_compile_variation": (C.c_int, [C.c_uint32, C.POINTER(C.c_uint64)]),

@@ -184,6 +184,7 @@ struct pyr3_renderer {
   float* d_knorm = nullptr;
   float* d_kwtab = nullptr;
   float* d_kern = nullptr;
+  float* d_curves = nullptr;  // 5 x 256 colour-curves LUT
   void* d_out = nullptr;
   size_t out_bytes = 0;
   uint16_t* d_pick = nullptr;
@@ -277,6 +278,7 @@ PYR3_API int pyr3_create(const pyr3_opts* opts, pyr3_renderer** out) {
   CUDA_TRY(cudaMalloc(&r->d_knorm, 257 * 4));
   CUDA_TRY(cudaMalloc(&r->d_kwtab, pyr3::kw_table_floats() * 4));
   CUDA_TRY(cudaMalloc(&r->d_kern, pyr3::kMaxTaps * 4));
+  CUDA_TRY(cudaMalloc(&r->d_curves, 5 * 256 * 4));
   CUDA_TRY(cudaMalloc(&r->d_counters, 16));
   CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, 16, r->stream));
   CUDA_TRY(cudaMalloc(&r->d_sched, 16));
@@ -304,6 +306,7 @@ PYR3_API int pyr3_destroy(pyr3_renderer* r) {
   cudaFree(r->d_knorm);
   cudaFree(r->d_kwtab);
   cudaFree(r->d_kern);
+  cudaFree(r->d_curves);
   cudaFree(r->d_pick);
   cudaFree(r->d_counters);
   cudaFree(r->d_sched);
@@ -600,8 +603,15 @@ static int run_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t to
   t.bg[1] = p->background[1];
   t.bg[2] = p->background[2];
   t.transparent = p->transparent;
-  CUDA_TRY(pyr3::launch_tonemap(filtered ? nullptr : r->d_hist, filtered, t, r->d_kern, dev_out,
-                                out_kind == PYR3_OUT_RGBA8, r->stream));
+  t.curves_active = p->curves ? (p->curves_active & 31u) : 0u;
+  if (t.curves_active)
+    CUDA_TRY(cudaMemcpyAsync(r->d_curves, p->curves, 5 * 256 * 4, cudaMemcpyHostToDevice, r->stream));
+  t.hsl_active = p->hsl_active ? 1u : 0u;
+  t.hsl_hue = p->hsl_hue;
+  t.hsl_sat = p->hsl_sat;
+  t.hsl_light = p->hsl_light;
+  CUDA_TRY(pyr3::launch_tonemap(filtered ? nullptr : r->d_hist, filtered, t, r->d_kern, r->d_curves,
+                                dev_out, out_kind == PYR3_OUT_RGBA8, r->stream));
   return PYR3_OK;
 }
 
@@ -643,6 +653,18 @@ PYR3_API int pyr3_read_histogram(pyr3_renderer* r, uint32_t* host_out) {
   cudaSetDevice(r->device);
   CUDA_TRY(cudaMemcpyAsync(host_out, r->d_hist, (size_t)r->SW * r->SH * 16, cudaMemcpyDeviceToHost,
                            r->stream));
+  return check_sched(r);
+}
+
+PYR3_API int pyr3_read_linear(pyr3_renderer* r, double k1, double k2, float* host_out) {
+  if (!r || !host_out) return fail(PYR3_E_INVALID, "null argument");
+  cudaSetDevice(r->device);
+  const size_t bytes = (size_t)r->W * r->H * 16;
+  int rc = ensure_out(r, bytes);
+  if (rc) return rc;
+  CUDA_TRY(pyr3::launch_linear_export(r->d_hist, r->W, r->H, r->os, k1, k2, (float*)r->d_out,
+                                      r->stream));
+  CUDA_TRY(cudaMemcpyAsync(host_out, r->d_out, bytes, cudaMemcpyDeviceToHost, r->stream));
   return check_sched(r);
 }
 
@@ -940,8 +962,15 @@ PYR3_API int pyr3_density_tonemap_noalloc(const uint32_t* device_hist, uint32_t 
   t.bg[1] = p->background[1];
   t.bg[2] = p->background[2];
   t.transparent = p->transparent;
-  CUDA_TRY(pyr3::launch_tonemap(filtered ? nullptr : device_hist, filtered, t, sc.kern, device_out,
-                                out_kind == PYR3_OUT_RGBA8, s));
+  t.curves_active = p->curves ? (p->curves_active & 31u) : 0u;
+  if (t.curves_active)
+    CUDA_TRY(cudaMemcpyAsync(sc.curves, p->curves, 5 * 256 * sizeof(float), cudaMemcpyHostToDevice, s));
+  t.hsl_active = p->hsl_active ? 1u : 0u;
+  t.hsl_hue = p->hsl_hue;
+  t.hsl_sat = p->hsl_sat;
+  t.hsl_light = p->hsl_light;
+  CUDA_TRY(pyr3::launch_tonemap(filtered ? nullptr : device_hist, filtered, t, sc.kern, sc.curves,
+                                device_out, out_kind == PYR3_OUT_RGBA8, s));
   return PYR3_OK;
 }
 

@@ -27,12 +27,13 @@ namespace {
 constexpr size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // Layout of the scratch array: kernel-norm LUT (257 f32), spatial-filter
-// taps, the exp-weight table of the density pass, then the density output
-// (f32 x 4 per super-sampled pixel).
+// taps, colour-curves LUT (5 x 256 f32), the exp-weight table of the density
+// pass, then the density output (f32 x 4 per super-sampled pixel).
 constexpr size_t kKwRegionFloats = 90112;  // >= kw_table_floats() (checked at set-up)
 constexpr size_t kOffKnorm = 0;
 constexpr size_t kOffKern = kOffKnorm + align256(257 * sizeof(float));
-constexpr size_t kOffKw = kOffKern + align256(kMaxTaps * sizeof(float));
+constexpr size_t kOffCurves = kOffKern + align256(kMaxTaps * sizeof(float));
+constexpr size_t kOffKw = kOffCurves + align256(5 * 256 * sizeof(float));
 constexpr size_t kOffFiltered = kOffKw + align256(kKwRegionFloats * sizeof(float));
 constexpr size_t kScratchBytes = kOffFiltered + kNoAllocMaxSuperPixels * 4 * sizeof(float);
 
@@ -49,8 +50,9 @@ const size_t kNoAllocScratchBytes = kScratchBytes;
 // Once per device (the current one): look up the array's device address --
 // in host code its name is only a host-side stand-in, not a device
 // address -- then fill the tables, which later calls only read.  Nothing
-// else in the array needs to start at zero: each call writes the taps and,
-// when density estimation is on, every density-output pixel it later reads.
+// else in the array needs to start at zero: each call writes the taps, the
+// curves LUT when it uses curves, and, when density estimation is on, every
+// density-output pixel it later reads.
 cudaError_t noalloc_scratch(const float* knorm_host, cudaStream_t stream, NoAllocScratch* out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -75,6 +77,7 @@ cudaError_t noalloc_scratch(const float* knorm_host, cudaStream_t stream, NoAllo
   out->knorm = (const float*)(base + kOffKnorm);
   out->kwtab = (const float*)(base + kOffKw);
   out->kern = (float*)(base + kOffKern);
+  out->curves = (float*)(base + kOffCurves);
   out->filtered = (float*)(base + kOffFiltered);
   return cudaSuccess;
 }

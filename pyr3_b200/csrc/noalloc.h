@@ -14,6 +14,7 @@ struct NoAllocScratch {
   const float* knorm;  // 257-entry kernel-norm LUT
   const float* kwtab;  // density exp-weight table
   float* kern;         // spatial-filter taps (written per call)
+  float* curves;       // colour-curves LUT, 5 x 256 f32 (written per call when used)
   float* filtered;     // density output, kNoAllocMaxSuperPixels x 4 f32
 };
 

@@ -17,7 +17,8 @@
 // visualize_u32.wgsl:147-248 and visualize_f32.wgsl:162-271): fw x fw
 // spatial-filter collapse of the super-res source (per-tap log-density ls
 // for the raw histogram), flam3 alpha / vibrancy / highlight-power
-// composite, background blend, clamp; curves and HSL adjustments are off.
+// composite, background blend, clamp, then the colour curves (5 x 256 LUT:
+// luma, r, g, b, composite, in the shader's order) and the HSL adjustment.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -204,10 +205,20 @@ __device__ __forceinline__ void calc_newrgb(const float c[3], float ls, float hi
   }
 }
 
+// Colour-curves lookup (visualize_u32.wgsl:51-56): linear between the two
+// nearest of 256 entries of channel ch.
+__device__ __forceinline__ float curve_lut(const float* __restrict__ lut, int ch, float x) {
+  const float idx = fminf(fmaxf(x, 0.0f), 1.0f) * 255.0f;
+  const unsigned i0 = (unsigned)floorf(idx);
+  const unsigned i1 = min(i0 + 1u, 255u);
+  const float t = idx - (float)i0;
+  return lut[ch * 256 + i0] * (1.0f - t) + lut[ch * 256 + i1] * t;
+}
+
 template <bool kU32, bool kRgba8>
 __global__ void __launch_bounds__(256)
 k_tonemap(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapParams p,
-          const float* __restrict__ kern, void* __restrict__ out) {
+          const float* __restrict__ kern, const float* __restrict__ curves, void* __restrict__ out) {
   __shared__ float kk[kMaxTaps];
   if (threadIdx.x < p.fwidth) kk[threadIdx.x] = kern[threadIdx.x];
   __syncthreads();
@@ -263,6 +274,34 @@ k_tonemap(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapPa
       const float bg = p.transparent ? 0.0f : (1.0f - alpha) * 256.0f * p.bg[i];
       o[i] = fminf(fmaxf((nrgb[i] + perch + bg) / 256.0f, 0.0f), 1.0f);
     }
+    if (p.curves_active) {  // visualize_u32.wgsl:217-231
+      if (p.curves_active & 16u) {
+        const float l = o[0] * 0.299f + o[1] * 0.587f + o[2] * 0.114f;
+        const float ln = curve_lut(curves, 4, l);
+        if (l > 0.0f) {
+          const float k = ln / l;
+          o[0] *= k; o[1] *= k; o[2] *= k;
+        }
+      }
+      if (p.curves_active & 2u) o[0] = curve_lut(curves, 1, o[0]);
+      if (p.curves_active & 4u) o[1] = curve_lut(curves, 2, o[1]);
+      if (p.curves_active & 8u) o[2] = curve_lut(curves, 3, o[2]);
+      if (p.curves_active & 1u) {
+        o[0] = curve_lut(curves, 0, o[0]);
+        o[1] = curve_lut(curves, 0, o[1]);
+        o[2] = curve_lut(curves, 0, o[2]);
+      }
+    }
+    if (p.hsl_active) {  // visualize_u32.wgsl:234-243
+      float hsv[3];
+      rgb2hsv(o, hsv);
+      hsv[0] = hsv[0] + p.hsl_hue;
+      hsv[0] = hsv[0] - 360.0f * floorf(hsv[0] / 360.0f);
+      hsv[1] = fminf(fmaxf(hsv[1] * p.hsl_sat, 0.0f), 1.0f);
+      hsv[2] = fminf(fmaxf(hsv[2] + p.hsl_light, 0.0f), 1.0f);
+      hsv2rgb(hsv, o);
+    }
+    for (int i = 0; i < 3; ++i) o[i] = fminf(fmaxf(o[i], 0.0f), 1.0f);
     o[3] = p.transparent ? alpha : 1.0f;
   }
   const size_t oi = (size_t)yi * p.width + xi;
@@ -294,15 +333,47 @@ cudaError_t launch_density(const uint32_t* hist, float* filtered, const DeParams
 }
 
 cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, const TonemapParams& p,
-                           const float* kern, void* out, bool rgba8, cudaStream_t s) {
+                           const float* kern, const float* curves, void* out, bool rgba8,
+                           cudaStream_t s) {
   dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
   if (hist_u32) {
-    if (rgba8) k_tonemap<true, true><<<grid, 256, 0, s>>>((const uint4*)hist_u32, nullptr, p, kern, out);
-    else k_tonemap<true, false><<<grid, 256, 0, s>>>((const uint4*)hist_u32, nullptr, p, kern, out);
+    if (rgba8) k_tonemap<true, true><<<grid, 256, 0, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out);
+    else k_tonemap<true, false><<<grid, 256, 0, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out);
   } else {
-    if (rgba8) k_tonemap<false, true><<<grid, 256, 0, s>>>(nullptr, (const float4*)filtered, p, kern, out);
-    else k_tonemap<false, false><<<grid, 256, 0, s>>>(nullptr, (const float4*)filtered, p, kern, out);
+    if (rgba8) k_tonemap<false, true><<<grid, 256, 0, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out);
+    else k_tonemap<false, false><<<grid, 256, 0, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out);
   }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------- linear export
+__global__ void __launch_bounds__(256)
+k_linear_export(const uint4* __restrict__ hist, uint32_t width, uint32_t height, uint32_t os,
+                double scale, float4* __restrict__ out) {
+  const uint32_t x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 16 + (threadIdx.x >> 4);
+  if (x >= width || y >= height) return;
+  const size_t sw = (size_t)width * os;
+  double r = 0.0, g = 0.0, b = 0.0, c = 0.0;  // integer sums: exact in f64
+  for (uint32_t sy = 0; sy < os; ++sy)
+    for (uint32_t sx = 0; sx < os; ++sx) {
+      const uint4 h = hist[((size_t)y * os + sy) * sw + (size_t)x * os + sx];
+      r += (double)h.x;
+      g += (double)h.y;
+      b += (double)h.z;
+      c += (double)h.w;
+    }
+  const double a = c * scale;
+  out[(size_t)y * width + x] = make_float4((float)(r * scale), (float)(g * scale), (float)(b * scale),
+                                           (float)(a < 0.0 ? 0.0 : (a > 1.0 ? 1.0 : a)));
+}
+
+cudaError_t launch_linear_export(const uint32_t* hist, uint32_t width, uint32_t height,
+                                 uint32_t oversample, double k1, double k2, float* out,
+                                 cudaStream_t s) {
+  const double scale = (k1 * k2) / (double)(oversample * oversample);
+  dim3 grid((width + 15) / 16, (height + 15) / 16);
+  k_linear_export<<<grid, 256, 0, s>>>((const uint4*)hist, width, height, oversample, scale,
+                                       (float4*)out);
   return cudaGetLastError();
 }
 

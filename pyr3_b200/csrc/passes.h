@@ -15,19 +15,31 @@ struct DeParams {
   int R;                   // ceil(clamp(max_rad, 0, 256))
 };
 
-// visualize uniforms (src/visualize.ts:178-204), curves/HSL off.
+// visualize uniforms (src/visualize.ts:178-204).
 struct TonemapParams {
   uint32_t width, height, oversample, fwidth;
   float k1, k2, gamma, vibrancy, highpow, linrange;
   float bg[3];
   int transparent;
+  uint32_t curves_active;  // channel-curves mask: composite 1, r 2, g 4, b 8, luma 16
+  uint32_t hsl_active;
+  float hsl_hue, hsl_sat, hsl_light;  // degrees, multiplier, addend
 };
 
 cudaError_t build_kw_table(const float* knorm, float* tab, cudaStream_t s);
 size_t kw_table_floats();
 cudaError_t launch_density(const uint32_t* hist, float* filtered, const DeParams& p,
                            const float* knorm, const float* tab, cudaStream_t s);
+// curves: 5 x 256 f32 LUT on the device (read only when p.curves_active != 0).
 cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, const TonemapParams& p,
-                           const float* kern, void* out, bool rgba8, cudaStream_t s);
+                           const float* kern, const float* curves, void* out, bool rgba8,
+                           cudaStream_t s);
+
+// histogramToLinearRgba (src/export-linear.ts:24-47): box-collapse of each
+// oversample x oversample block in f64, scaled by k1 * k2 / oversample^2;
+// coverage (alpha) clamped to [0, 1].  out = width x height x RGBA f32.
+cudaError_t launch_linear_export(const uint32_t* hist, uint32_t width, uint32_t height,
+                                 uint32_t oversample, double k1, double k2, float* out,
+                                 cudaStream_t s);
 
 }  // namespace pyr3

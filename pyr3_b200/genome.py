@@ -96,6 +96,8 @@ class Genome:
     filter_radius: float | None = None
     background: tuple = (0.0, 0.0, 0.0)
     palette_mode: str = "step"  # splat-time palette sampling: step | linear
+    channel_curves: dict | None = None  # {composite, r, g, b, luma: [(x, y), ...]}
+    hsl_adjust: dict | None = None  # {hue (degrees), sat (percent), light (percent)}
 
 
 DEFAULT_TONEMAP = {"gamma": 2.4, "vibrancy": 0.0, "highlightPower": 1.0, "brightness": 1.0,
@@ -156,6 +158,11 @@ def genome_from_json(j) -> Genome:
     if j.get("background"):
         g.background = tuple(float(c) for c in j["background"])
     g.palette_mode = j.get("paletteMode", "step")
+    if j.get("channelCurves"):
+        g.channel_curves = {ch: [(float(p["x"]), float(p["y"])) for p in pts]
+                            for ch, pts in j["channelCurves"].items()}
+    if j.get("hslAdjust"):
+        g.hsl_adjust = {k: float(v) for k, v in j["hslAdjust"].items()}
     return g
 
 
@@ -395,4 +402,64 @@ def bake_lut(stops, hue: float = 0.0, mode: str = "linear") -> np.ndarray:
             else:
                 rgb = [L[c] + (H[c] - L[c]) * u for c in (1, 2, 3)]
         out[i * 4:i * 4 + 3] = rgb
+    return out
+
+
+# ------------------------------------------------------------ colour curves
+# src/channel-curves.ts: five 256-entry LUTs (composite, r, g, b, luma) and
+# the bit mask of the channels that are not the identity.
+CURVE_CHANNELS = ("composite", "r", "g", "b", "luma")
+
+
+def _curve_is_identity(pts) -> bool:
+    return len(pts) == 2 and tuple(pts[0]) == (0, 0) and tuple(pts[1]) == (1, 1)
+
+
+def curves_active_mask(curves) -> int:
+    """channel-curves.ts activeMask: bit i set when channel i is not identity."""
+    if not curves:
+        return 0
+    return sum(1 << i for i, ch in enumerate(CURVE_CHANNELS)
+               if not _curve_is_identity(curves.get(ch, [(0, 0), (1, 1)])))
+
+
+def eval_curve(pts, x: float) -> float:
+    """Catmull-Rom (B = 0.5) through the control points with duplicated
+    end neighbours, clamped to the end values (channel-curves.ts evalCurve)."""
+    first, last = pts[0], pts[-1]
+    if x <= first[0]:
+        return first[1]
+    if x >= last[0]:
+        return last[1]
+    if len(pts) < 3:
+        dx = pts[1][0] - first[0]
+        if dx < 1e-9:
+            return first[1]
+        return first[1] + (x - first[0]) / dx * (pts[1][1] - first[1])
+    i = 0
+    while i < len(pts) - 1 and pts[i + 1][0] < x:
+        i += 1
+    xa, xb = pts[max(0, i - 1)][1], pts[i][1]
+    xc, xd = pts[i + 1][1], pts[min(len(pts) - 1, i + 2)][1]
+    seg = pts[i + 1][0] - pts[i][0]
+    if seg < 1e-9:
+        return xb
+    u = (x - pts[i][0]) / seg
+    bb = 0.5
+    c = u * u * u * (-bb * xa + (2 - bb) * xb + (bb - 2) * xc + bb * xd)
+    c += u * u * (2 * bb * xa + (bb - 3) * xb + (3 - 2 * bb) * xc - bb * xd)
+    c += u * (-bb * xa + bb * xc)
+    return c + xb
+
+
+def bake_curves(curves) -> np.ndarray | None:
+    """5 x 256 f32 LUT (channel-curves.ts bakeCurves), None when every
+    channel is the identity."""
+    if curves_active_mask(curves) == 0:
+        return None
+    out = np.zeros(5 * 256, np.float32)
+    for ch, name in enumerate(CURVE_CHANNELS):
+        pts = curves.get(name, [(0, 0), (1, 1)])
+        for i in range(256):
+            out[ch * 256 + i] = min(1.0, max(0.0, eval_curve(pts, i / 255)))
     return out

@@ -16,8 +16,8 @@ import math
 import numpy as np
 
 from . import _lib
-from .genome import (DEFAULT_TONEMAP, Genome, bake_lut, expand_for_gpu, final_slot, pack_xforms,
-                     xaos_matrix)
+from .genome import (DEFAULT_TONEMAP, Genome, bake_curves, bake_lut, curves_active_mask,
+                     expand_for_gpu, final_slot, pack_xforms, xaos_matrix)
 
 # src/renderer.ts:23-47
 DEFAULT_FILTER_RADIUS = 0.5
@@ -139,12 +139,23 @@ class Renderer:
         tm.update(genome.tonemap or {})
         de = genome.density
         use_de = de is not None and not force_de_off
-        return _lib.PresentOpts(
+        p = _lib.PresentOpts(
             tm["gamma"], tm["vibrancy"], tm["highlightPower"], tm["brightness"],
             tm["gammaThreshold"], 1 if use_de else 0,
             de["maxRad"] if use_de else 0.0, de["minRad"] if use_de else 0.0,
             de["curve"] if use_de else 0.0, (C.c_float * 3)(*genome.background),
             1 if transparent else 0, float(genome.scale))
+        lut = bake_curves(genome.channel_curves)
+        if lut is not None:  # src/visualize.ts:170-175
+            p.curves_active = curves_active_mask(genome.channel_curves)
+            p.curves = lut.ctypes.data
+            p._curves_lut = lut  # keeps the LUT alive as long as the struct
+        if genome.hsl_adjust:  # src/visualize.ts:194-198
+            p.hsl_active = 1
+            p.hsl_hue = genome.hsl_adjust.get("hue", 0.0)
+            p.hsl_sat = genome.hsl_adjust.get("sat", 100.0) / 100.0
+            p.hsl_light = genome.hsl_adjust.get("light", 0.0) / 100.0
+        return p
 
     def present(self, genome: Genome, total_samples: int, force_de_off: bool = False,
                 transparent: bool = False, out: np.ndarray | None = None,
@@ -178,6 +189,18 @@ class Renderer:
         h = np.zeros((self.super_h, self.super_w, 4), np.uint32)
         _lib.check(_lib.lib().pyr3_read_histogram(self._h, _lib.ptr(h)))
         return h, self.super_w, self.super_h
+
+    def read_linear(self, genome: Genome, total_samples: int) -> np.ndarray:
+        """Linear scene-referred RGBA f32 [H, W, 4] of the histogram
+        (src/export-linear.ts:24-47, the exr-linear export), k1 and k2 from
+        deriveCalibration (src/calibration.ts:37-43) in double."""
+        tm = dict(DEFAULT_TONEMAP)
+        tm.update(genome.tonemap or {})
+        k1 = (tm["brightness"] * 255.0 * 268.0) / 256.0
+        k2 = (self.oversample ** 2 * genome.scale * genome.scale) / (255.0 * total_samples)
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        _lib.check(_lib.lib().pyr3_read_linear(self._h, k1, k2, _lib.ptr(out)))
+        return out
 
     def set_capture_index(self, on: bool) -> None:
         _lib.check(_lib.lib().pyr3_set_capture_index(self._h, 1 if on else 0))

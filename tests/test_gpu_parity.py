@@ -269,6 +269,48 @@ def test_density_tonemap_within_1_255(os_, de):
     assert float(np.abs(out - ref).max()) <= 1.0 / 255.0
 
 
+def test_tonemap_curves_and_hsl_within_1_255():
+    """Colour curves (composite, r, b, luma) + HSL adjustment on a DE'd
+    histogram: device tonemap vs the oracle's visualize within 1/255."""
+    W, H, os_ = 160, 120, 2
+    g, _, hist, samples = _c1_histogram(W * os_, H * os_)
+    g.scale = W / 4
+    g.channel_curves = {"composite": [(0, 0.05), (0.5, 0.6), (1, 1)], "r": [(0, 0), (1, 0.9)],
+                        "b": [(0, 0.1), (0.3, 0.2), (0.7, 0.8), (1, 1)],
+                        "luma": [(0, 0), (0.4, 0.5), (1, 1)]}
+    g.hsl_adjust = {"hue": 37.0, "sat": 130.0, "light": -5.0}
+    p = R.Renderer.present_opts(None, g)
+    assert p.curves_active == 0b11011 and p.hsl_active == 1
+    out = np.zeros(W * H * 4, np.float32)
+    _lib.check(_lib.lib().pyr3_density_tonemap(_lib.ptr(hist), W, H, os_, 0.5, C.byref(p), samples,
+                                               _lib.ptr(out), None))
+    k1, k2 = O.derive_calibration(g.scale, samples, 4.0, os_)
+    filt = O.density(hist, W * os_, H * os_, 9.0 * os_ + 1, 1.0, 0.4, np.float32(k1), np.float32(k2))
+    ref = O.visualize(W, H, os_, O.spatial_kernel(0.5, os_), np.float32(k1), np.float32(k2), 4.0, 1.0,
+                      1.0, 0.01, src_f32=filt, curves_active=p.curves_active,
+                      curves=G.bake_curves(g.channel_curves), hsl=(37.0, 1.3, -0.05))
+    assert float(np.abs(out - ref).max()) <= 1.0 / 255.0
+
+
+def test_linear_export_bit_exact():
+    """histogramToLinearRgba (src/export-linear.ts:24-47) on the device:
+    f64 box-collapse and k1*k2 scaling equal the oracle bit for bit."""
+    W, H, os_ = 160, 120, 2
+    g = workloads.plain_small()
+    g.scale = W / 4
+    r = R.create_renderer(W, H, os_)
+    r.reset(g)
+    r.iterate(g, seed=4, walkers=1024, iters_per_walker=4000)
+    samples, _ = r.counters()
+    hist, _, _ = r.read_histogram()
+    got = r.read_linear(g, samples)
+    k1, k2 = O.derive_calibration(g.scale, samples, 4.0, os_)
+    want = O.histogram_to_linear(hist.reshape(-1), W, H, os_, k1, k2).reshape(H, W, 4)
+    assert np.array_equal(got, want)
+    assert float(got[..., 3].max()) > 0.0
+    r.destroy()
+
+
 # ---------------------------------------------------- whole-render statistics
 def _collapse(hist, W, H, os_):
     h = hist.reshape(H * os_, W * os_, 4).astype(np.float64)

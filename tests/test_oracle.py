@@ -178,3 +178,66 @@ def test_density_and_visualize_restatement_match_reference():
     v1 = O.visualize(*args, src_f32=a)
     v2 = O.ref_visualize(*args, src_f32=a)
     assert np.array_equal(v1, v2)
+
+
+def _curves_and_hsl():
+    from pyr3_b200 import genome as G
+
+    curves = {"composite": [(0, 0.05), (0.5, 0.6), (1, 1)], "r": [(0, 0), (1, 0.9)],
+              "g": [(0, 0), (1, 1)], "b": [(0, 0.1), (0.3, 0.2), (0.7, 0.8), (1, 1)],
+              "luma": [(0, 0), (0.4, 0.5), (1, 1)]}
+    return G.bake_curves(curves), G.curves_active_mask(curves), (37.0, 1.3, -0.05)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference shaders not compiled here")
+def test_visualize_curves_and_hsl_restatement_matches_reference():
+    """oracle.c's colour curves + HSL adjustment (visualize_u32.wgsl:217-243)
+    equal the reference's WGSL on the CPU, for u32 and f32 sources."""
+    rng = np.random.default_rng(6)
+    W, H = 48, 40
+    hist = np.zeros((H, W, 4), np.uint32)
+    cnt = rng.integers(0, 9, (H, W)) * 255
+    cnt[rng.random((H, W)) < 0.3] = 0
+    hist[..., 3] = cnt
+    for ch in range(3):
+        hist[..., ch] = (cnt * rng.random((H, W))).astype(np.uint32)
+    hist = hist.reshape(-1)
+    k1, k2 = O.derive_calibration(40, 5e4, 4)
+    lut, mask, hsl = _curves_and_hsl()
+    assert mask == 0b11011
+    kern = O.spatial_kernel(0.5, 2)
+    args = (W // 2, H // 2, 2, kern, k1, k2, 4.0, 1.0, 1.0, 0.01)
+    for kw in ({"curves_active": mask, "curves": lut}, {"hsl": hsl},
+               {"curves_active": mask, "curves": lut, "hsl": hsl}):
+        v1 = O.visualize(*args, src_u32=hist, **kw)
+        v2 = O.ref_visualize(*args, src_u32=hist, **kw)
+        assert np.array_equal(v1, v2), kw
+        assert not np.array_equal(v1, O.visualize(*args, src_u32=hist))
+    a = O.density(hist, W, H, 10.0, 1.0, 0.4, k1, k2)
+    kw = {"curves_active": mask, "curves": lut, "hsl": hsl}
+    assert np.array_equal(O.visualize(*args, src_f32=a, **kw), O.ref_visualize(*args, src_f32=a, **kw))
+
+
+def test_bake_curves_matches_reference_cases():
+    """src/channel-curves.test.ts: activeMask bits, identity / inverse
+    bakes, end clamps."""
+    from pyr3_b200 import genome as G
+
+    ident = [(0, 0), (1, 1)]
+    lift = [(0, 0.1), (1, 1)]
+    assert G.curves_active_mask(None) == 0
+    names = G.CURVE_CHANNELS
+    assert G.curves_active_mask({n: ident for n in names}) == 0
+    for i, n in enumerate(names):
+        assert G.curves_active_mask({m: (lift if m == n else ident) for m in names}) == 1 << i
+    assert G.curves_active_mask({n: lift for n in names}) == 0b11111
+    one = {n: ident for n in names}
+    one["composite"] = [(0, 1), (1, 0)]
+    lut = G.bake_curves(one)
+    assert np.allclose(lut[:256], 1 - np.arange(256) / 255, atol=5e-3)
+    assert np.allclose(lut[256:512], np.arange(256) / 255, atol=5e-3)
+    one["composite"] = [(0.25, 0.5), (1, 1)]
+    lut = G.bake_curves(one)
+    assert lut[0] == pytest.approx(0.5, abs=1e-3) and lut[63] == pytest.approx(0.5, abs=1e-3)
+    one["composite"] = [(0, 0), (0.75, 0.5)]
+    assert G.bake_curves(one)[200] == pytest.approx(0.5, abs=1e-3)
