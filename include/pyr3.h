@@ -114,6 +114,8 @@ typedef struct {
 #define PYR3_OUT_RGBA8 0      /* W x H x 4 u8 (rgba8unorm) */
 #define PYR3_OUT_RGBA32F 1    /* W x H x 4 f32 (fragment value) */
 
+typedef struct pyr3_batch pyr3_batch;
+
 /* ---- lifecycle -------------------------------------------------------- */
 /* createRenderer (src/renderer.ts:214). */
 int pyr3_create(const pyr3_opts *opts, pyr3_renderer **out);
@@ -148,6 +150,24 @@ int pyr3_read_histogram(pyr3_renderer *r, uint32_t *host_out);
  * histogram, computed on the device: width x height x RGBA f32 linear,
  * scene-referred values (k1, k2 from deriveCalibration, src/calibration.ts). */
 int pyr3_read_linear(pyr3_renderer *r, double k1, double k2, float *host_out);
+/* ---- batches ---------------------------------------------------------- */
+/* Batched rendering of many genomes in one CUDA graph (the north_star's
+ * batched persistent launch; no counterpart in the reference, which renders
+ * genomes one dispatch at a time).  renderers[i] renders genomes[i] with
+ * opts[i] (walkers x iters_per_walker samples; without
+ * PYR3_ITER_EXACT_WALKERS the batch picks its own walker count per genome).
+ * All renderers must be on one device.  pyr3_batch_run clears every
+ * renderer's histogram and accumulates its samples, asynchronously, on the
+ * batch's own stream; after pyr3_batch_sync each renderer can be presented
+ * or read.  Genome values are captured at creation. */
+int pyr3_batch_create(pyr3_renderer *const *renderers, const pyr3_genome *genomes,
+                      const pyr3_iterate_opts *opts, uint32_t n, uint32_t n_streams,
+                      pyr3_batch **out);
+int pyr3_batch_run(pyr3_batch *b);
+/* Wait for the last run; its device time (ms) and total samples. */
+int pyr3_batch_sync(pyr3_batch *b, float *ms, uint64_t *samples);
+int pyr3_batch_destroy(pyr3_batch *b);
+
 /* Renderer.readIndexMap (src/renderer.ts:205): superW*superH u32 colour
  * index sums (valid after iterating with capture on). */
 int pyr3_read_index_map(pyr3_renderer *r, uint32_t *host_out);

@@ -105,6 +105,11 @@ _SIGS = {
                                                C.c_void_p, C.c_int32, C.c_void_p]),
     "pyr3_prepare": (C.c_int, [C.c_void_p, C.POINTER(GenomeC)]),
     "pyr3_read_linear": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p]),
+    "pyr3_batch_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                    C.POINTER(C.c_void_p)]),
+    "pyr3_batch_run": (C.c_int, [C.c_void_p]),
+    "pyr3_batch_sync": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint64)]),
+    "pyr3_batch_destroy": (C.c_int, [C.c_void_p]),
     "pyr3_jit_compile": (C.c_int, [C.POINTER(GenomeC), C.c_int32, C.POINTER(C.c_uint64)]),
     "pyr3_jit_source": (C.c_int, [C.POINTER(GenomeC), C.c_char_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     "pyr3_jit_compile_variation": (C.c_int, [C.c_uint32, C.POINTER(C.c_uint64)]),

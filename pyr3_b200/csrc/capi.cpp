@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -434,16 +435,13 @@ int launch_chaos(pyr3_renderer* r, const pyr3::ChaosModule& m, bool queue, Chaos
 }
 }  // namespace
 
-PYR3_API int pyr3_iterate(pyr3_renderer* r, const pyr3_genome* g, const pyr3_iterate_opts* o) {
-  if (!r || !g || !o) return fail(PYR3_E_INVALID, "null argument");
-  cudaSetDevice(r->device);
-  const bool aggregate = (o->flags & PYR3_ITER_AGGREGATE) != 0;
-  std::shared_ptr<pyr3::ChaosModule> m;
-  int rc = prepare_module(r, g, aggregate, &m);
-  if (rc) return rc;
+namespace {
+// Upload a genome's pick-table boundaries (renderer-owned buffer) and its
+// packed xform records (the module's constant bank), on the renderer's
+// stream.
+int upload_genome(pyr3_renderer* r, const pyr3_genome* g, pyr3::ChaosModule& m) {
   const int n = (int)g->n_xforms;
   const bool has_final = g->final_slot >= 0;
-  // pick table boundaries
   std::vector<float> weights(n);
   for (int i = 0; i < n; ++i) weights[i] = g->xforms[(size_t)i * 116 + 3];
   std::vector<uint16_t> starts;
@@ -459,11 +457,14 @@ PYR3_API int pyr3_iterate(pyr3_renderer* r, const pyr3_genome* g, const pyr3_ite
   }
   CUDA_TRY(cudaMemcpyAsync(r->d_pick, starts.data(), pick_bytes, cudaMemcpyHostToDevice, r->stream));
   const size_t xf_bytes = (size_t)(n + (has_final ? 1 : 0)) * 116 * 4;
-  if (xf_bytes > m->c_xf_bytes) return fail(PYR3_E_INVALID, "xform records exceed module constant bank");
-  CUDA_TRY(cudaMemcpyAsync(m->c_xf, g->xforms, xf_bytes, cudaMemcpyHostToDevice, r->stream));
+  if (xf_bytes > m.c_xf_bytes) return fail(PYR3_E_INVALID, "xform records exceed module constant bank");
+  CUDA_TRY(cudaMemcpyAsync(m.c_xf, g->xforms, xf_bytes, cudaMemcpyHostToDevice, r->stream));
+  return PYR3_OK;
+}
 
-  const uint64_t total = o->walkers * o->iters_per_walker;
-  if (total == 0) return PYR3_OK;
+// Launch arguments of a chaos kernel that do not depend on the walker split
+// (chaos uniforms, src/chaos.ts:381-456).
+ChaosArgs base_args(pyr3_renderer* r, const pyr3_genome* g, const pyr3_iterate_opts* o) {
   ChaosArgs A;
   std::memset(&A, 0, sizeof A);
   A.hist = r->d_hist;
@@ -502,6 +503,23 @@ PYR3_API int pyr3_iterate(pyr3_renderer* r, const pyr3_genome* g, const pyr3_ite
   A.xform_blend = std::min(1.0f, std::max(0.0f, g->xform_blend));
   A.counters = r->d_counters;
   A.sched = r->d_sched;
+
+  return A;
+}
+}  // namespace
+
+PYR3_API int pyr3_iterate(pyr3_renderer* r, const pyr3_genome* g, const pyr3_iterate_opts* o) {
+  if (!r || !g || !o) return fail(PYR3_E_INVALID, "null argument");
+  cudaSetDevice(r->device);
+  const bool aggregate = (o->flags & PYR3_ITER_AGGREGATE) != 0;
+  std::shared_ptr<pyr3::ChaosModule> m;
+  int rc = prepare_module(r, g, aggregate, &m);
+  if (rc) return rc;
+  rc = upload_genome(r, g, *m);
+  if (rc) return rc;
+  const uint64_t total = o->walkers * o->iters_per_walker;
+  if (total == 0) return PYR3_OK;
+  ChaosArgs A = base_args(r, g, o);
 
   const bool exact = (o->flags & PYR3_ITER_EXACT_WALKERS) != 0;
   uint64_t done = 0, walker_base = 0, used = 0;
@@ -559,6 +577,171 @@ PYR3_API int pyr3_last_iterate_ms(pyr3_renderer* r, float* ms) {
   if (!r || !ms) return fail(PYR3_E_INVALID, "null argument");
   CUDA_TRY(cudaEventSynchronize(r->ev1));
   CUDA_TRY(cudaEventElapsedTime(ms, r->ev0, r->ev1));
+  return PYR3_OK;
+}
+
+// ------------------------------------------------------------------ batch
+// Many renderers, each with its own genome and iterate request, rendered by
+// one CUDA graph: every genome gets its own instance of its specialised
+// module (its own constant bank, so genomes of one structure do not collide)
+// and the graph clears each renderer's histogram and runs each genome's
+// chaos kernel, spread over worker streams so the launches run
+// concurrently.  Walkers per genome are chosen for the batch: enough
+// iterations per walker to keep the 200-iteration burn-in under ~10 %,
+// since the GPU is filled by running many genomes at once.
+struct pyr3_batch {
+  int device = 0;
+  cudaStream_t origin = nullptr;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> joins;
+  cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+  std::vector<std::shared_ptr<pyr3::ChaosModule>> mods;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t samples = 0;
+};
+
+namespace {
+constexpr uint64_t kBatchItersPerWalker = 2000;
+
+void free_batch(pyr3_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto s : b->streams) cudaStreamDestroy(s);
+  for (auto e : b->joins) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  delete b;
+}
+}  // namespace
+
+PYR3_API int pyr3_batch_create(pyr3_renderer* const* renderers, const pyr3_genome* genomes,
+                               const pyr3_iterate_opts* opts, uint32_t n, uint32_t n_streams,
+                               pyr3_batch** out) {
+  if (!renderers || !genomes || !opts || !out || n == 0 || n_streams == 0)
+    return fail(PYR3_E_INVALID, "bad arguments");
+  const int dev = renderers[0] ? renderers[0]->device : 0;
+  for (uint32_t i = 0; i < n; ++i)
+    if (!renderers[i] || renderers[i]->device != dev)
+      return fail(PYR3_E_INVALID, "batch renderers must be non-null and on one device");
+  cudaSetDevice(dev);
+  std::unique_ptr<pyr3_batch, void (*)(pyr3_batch*)> b(new pyr3_batch(), free_batch);
+  b->device = dev;
+  CUDA_TRY(cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreate(&b->ev0));
+  CUDA_TRY(cudaEventCreate(&b->ev1));
+  const uint32_t k = std::min(n_streams, n);
+  for (uint32_t j = 0; j < k; ++j) {
+    cudaStream_t st;
+    cudaEvent_t ev;
+    CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    b->streams.push_back(st);
+    CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    b->joins.push_back(ev);
+  }
+  // Modules (one instance per genome of a repeated structure), tables and
+  // records, and the launch arguments.
+  std::map<std::string, int> seen;
+  std::vector<ChaosArgs> args(n);
+  std::vector<unsigned> grids(n);
+  const int sms = device_sms(dev);
+  for (uint32_t i = 0; i < n; ++i) {
+    pyr3_renderer* r = renderers[i];
+    const pyr3_genome* g = &genomes[i];
+    const pyr3_iterate_opts* o = &opts[i];
+    if (!g->xforms) return fail(PYR3_E_INVALID, "null genome in batch");
+    pyr3::GenomeShape shape;
+    std::string e = pyr3::shape_from_packed(g->xforms, (int)g->n_xforms, g->final_slot, &shape);
+    if (!e.empty())
+      return fail(e.find("not implemented") != std::string::npos ? PYR3_E_UNSUPPORTED : PYR3_E_INVALID, e);
+    const bool aggregate = (o->flags & PYR3_ITER_AGGREGATE) != 0;
+    const std::string key = shape.key() + (aggregate ? "|A" : "");
+    const int inst = seen[key]++;
+    std::shared_ptr<pyr3::ChaosModule> m;
+    std::string err;
+    int rc = pyr3::get_chaos_module(shape, kWpb, aggregate, &m, &err, inst);
+    if (rc) return fail(rc, err);
+    b->mods.push_back(m);
+    rc = upload_genome(r, g, *m);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(r->stream));
+    const uint64_t total = o->walkers * o->iters_per_walker;
+    ChaosArgs A = base_args(r, g, o);
+    uint64_t nw;
+    if (o->flags & PYR3_ITER_EXACT_WALKERS) {
+      nw = std::max<uint64_t>(1, o->walkers);
+    } else {
+      const uint64_t cap = (uint64_t)m->blocks_per_sm * sms * m->wpb;
+      nw = std::max<uint64_t>(1, std::min<uint64_t>(cap, std::max<uint64_t>(256, total / kBatchItersPerWalker)));
+      nw = std::min<uint64_t>(nw, std::max<uint64_t>(1, total));
+    }
+    A.walker_base = 0;
+    A.n_walkers = nw;
+    A.iters_base = total / nw;
+    A.iters_extra = total % nw;
+    args[i] = A;
+    grids[i] = (unsigned)std::min<uint64_t>((nw + m->wpb - 1) / m->wpb, (uint64_t)m->blocks_per_sm * sms);
+    b->samples += total;
+  }
+  // Capture: fork to the worker streams, per genome clear + chaos kernel,
+  // join back.
+  CUDA_TRY(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+  cudaError_t ce = cudaEventRecord(b->fork, b->origin);
+  for (uint32_t j = 0; j < k && ce == cudaSuccess; ++j) ce = cudaStreamWaitEvent(b->streams[j], b->fork, 0);
+  for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
+    pyr3_renderer* r = renderers[i];
+    cudaStream_t st = b->streams[i % k];
+    ce = cudaMemsetAsync(r->d_hist, 0, (size_t)r->SW * r->SH * 16, st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(r->d_counters, 0, 16, st);
+    if (ce == cudaSuccess) {
+      void* params[] = {&args[i]};
+      ce = cudaLaunchKernel((const void*)b->mods[i]->chaos, dim3(grids[i]), dim3(b->mods[i]->wpb), params,
+                            b->mods[i]->smem, st);
+    }
+  }
+  for (uint32_t j = 0; j < k && ce == cudaSuccess; ++j) {
+    ce = cudaEventRecord(b->joins[j], b->streams[j]);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->origin, b->joins[j], 0);
+  }
+  cudaGraph_t graph = nullptr;
+  cudaError_t ee = cudaStreamEndCapture(b->origin, &graph);
+  if (ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return fail(PYR3_E_CUDA, std::string("batch capture: ") + cudaGetErrorString(ce));
+  }
+  if (ee != cudaSuccess) return fail(PYR3_E_CUDA, std::string("batch capture: ") + cudaGetErrorString(ee));
+  b->graph = graph;
+  CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  *out = b.release();
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_batch_run(pyr3_batch* b) {
+  if (!b) return fail(PYR3_E_INVALID, "null batch");
+  cudaSetDevice(b->device);
+  CUDA_TRY(cudaEventRecord(b->ev0, b->origin));
+  CUDA_TRY(cudaGraphLaunch(b->exec, b->origin));
+  CUDA_TRY(cudaEventRecord(b->ev1, b->origin));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_batch_sync(pyr3_batch* b, float* ms, uint64_t* samples) {
+  if (!b) return fail(PYR3_E_INVALID, "null batch");
+  cudaSetDevice(b->device);
+  CUDA_TRY(cudaEventSynchronize(b->ev1));
+  if (ms) CUDA_TRY(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+  if (samples) *samples = b->samples;
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_batch_destroy(pyr3_batch* b) {
+  if (!b) return PYR3_OK;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->origin);
+  free_batch(b);
   return PYR3_OK;
 }
 

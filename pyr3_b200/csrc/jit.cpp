@@ -270,8 +270,9 @@ std::string shape_from_packed(const float* xforms, int n, int final_slot, Genome
 }
 
 int get_chaos_module(const GenomeShape& s, int wpb, bool aggregate,
-                     std::shared_ptr<ChaosModule>* out, std::string* err) {
-  const std::string key = s.key() + "|w" + std::to_string(wpb) + (aggregate ? "|A" : "");
+                     std::shared_ptr<ChaosModule>* out, std::string* err, int instance) {
+  const std::string key = s.key() + "|w" + std::to_string(wpb) + (aggregate ? "|A" : "") +
+                          (instance > 0 ? "|i" + std::to_string(instance) : "");
   {
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_chaos_cache.find(key);

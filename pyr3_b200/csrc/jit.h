@@ -75,8 +75,10 @@ struct EvalModule {
 
 // Compile (or load from the in-process / on-disk cache) the chaos module.
 // Returns 0 or a PYR3_E_* code with *err set.
+// instance > 0 loads a separate copy of the module (its own __constant__
+// xform bank), for batches holding several genomes of one structure.
 int get_chaos_module(const GenomeShape& s, int wpb, bool aggregate,
-                     std::shared_ptr<ChaosModule>* out, std::string* err);
+                     std::shared_ptr<ChaosModule>* out, std::string* err, int instance = 0);
 // Generate and compile (no device needed) the chaos module source; returns
 // the cubin size through *bytes.  Used by CPU-side build checks.
 int compile_chaos_only(const GenomeShape& s, int wpb, bool aggregate, size_t* bytes,
