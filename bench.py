@@ -234,6 +234,7 @@ def bench_ours(args, ws, rank, local, dist):
     _barrier(dist)
     clocks = Clocks(local) if rank == 0 else None
     total_ms, chaos_ms = 0.0, []
+    launches0 = r.launches
     for k in range(args.steps):
         _lib.check(lib.pyr3_flush_l2(h, L2_FLUSH))
         _lib.check(lib.pyr3_mark(h, 0))
@@ -245,6 +246,7 @@ def bench_ours(args, ws, rank, local, dist):
         _lib.check(lib.pyr3_elapsed(h, 4, 5, C.byref(ms)))
         chaos_ms.append(ms.value)
     clk = clocks.stop() if clocks else None
+    chaos_launches = r.launches - launches0
     n_samples, n_splats = r.counters()
     _barrier(dist)
     t_max = _max_over_ranks(total_ms, dist, local)
@@ -278,12 +280,16 @@ def bench_ours(args, ws, rank, local, dist):
     value = ws * samples * args.steps / (t_max / 1e3)
     e2e = ws * samples * args.steps / (e2e_max / 1e3)
     peak, peak_kind = _peaks()
-    # Dominant kernel: the chaos kernel.  Algorithmic bytes per launch: every
-    # in-canvas splat reads and writes one 16-byte RGBA u32 bucket.  The
-    # counters restart at every reset, so they hold the last timed step.
-    splats_per_launch = n_splats
+    # Dominant kernel: the chaos kernel.  Algorithmic bytes: every in-canvas
+    # splat reads and writes one 16-byte RGBA u32 bucket.  The counters
+    # restart at every reset, so they hold the last timed step.  The wave
+    # kernel advances every walker one iteration per launch, so a step is
+    # many launches: bytes per launch / mean launch time = bytes per step /
+    # chaos time per step (the time between the launches counted in).
+    per_step_launches = max(1, chaos_launches // max(1, args.steps))
+    splats_per_launch = n_splats / per_step_launches
     mean_chaos = statistics.mean(chaos_ms)
-    achieved = splats_per_launch * 32.0 / (mean_chaos / 1e3) / 1e9
+    achieved = n_splats * 32.0 / (mean_chaos / 1e3) / 1e9
     traffic = None  # DRAM bytes per launch measured by ncu for this workload at full size
     tpath = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "roofline_traffic.json")
     if not args.samples and os.path.exists(tpath):
@@ -307,11 +313,11 @@ def bench_ours(args, ws, rank, local, dist):
         "chaos_kernel_ms": mean_chaos,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "note": f"chaos kernel; algorithmic bytes = 32 B (16 B bucket read+write) per "
-                             f"in-canvas splat ({splats_per_launch} splats per launch); peak {peak_kind}; "
-                             f"the kernel is bound by instruction issue and latency (ncu), not by HBM"},
-        "gpu_launches": args.steps * ((8 if g_close is not None else 1) + 1 +
-                                      (1 if g.density is not None else 0)),
+                     "note": f"chaos kernel, {per_step_launches} launches per step; algorithmic bytes = "
+                             f"32 B (16 B bucket read+write) per in-canvas splat ({splats_per_launch:.0f} "
+                             f"splats per launch); peak {peak_kind}; the kernel is bound by instruction "
+                             f"issue and latency (ncu), not by HBM"},
+        "gpu_launches": chaos_launches + args.steps * (1 + (1 if g.density is not None else 0)),
         "clocks": clk,
     }
     if ws == 1 and not args.no_cpu_baseline:
@@ -356,6 +362,21 @@ def bench_batch(args, ws, rank, local, dist):
             b.present(i)
         e2e_ms += (_t.perf_counter() - t0) * 1e3
     e2e_max = _max_over_ranks(e2e_ms, dist, local)
+    # The same genomes one after another through the per-genome path
+    # (pyr3_iterate, autotuned kernel), device time; the first pass loads
+    # the modules and runs the autotuner, the second is the one reported.
+    from pyr3_b200.renderer import compute_dispatch
+
+    seq_ms = 0.0
+    for _ in range(2):
+        seq_ms = 0.0
+        for i, g in enumerate(gs):
+            r = b.renderers[i]
+            w, it, _n = compute_dispatch(g.quality or 16, *g.size)
+            r.reset(g)
+            r.iterate(b.gpu[i], seed=11 + i, walkers=w, iters_per_walker=it)
+            seq_ms += r.last_iterate_ms()
+    seq_max = _max_over_ranks(seq_ms, dist, local)
     b.destroy()
     if rank != 0:
         return None
@@ -376,6 +397,9 @@ def bench_batch(args, ws, rank, local, dist):
                 "note": "graph launch + per-genome tonemap and RGBA8 readback; genomes uploaded once"},
         "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
                      "traffic": None, "note": f"chaos kernels bound by issue/latency; peak {peak_kind}"},
+        "per_genome_path": {"value": ws * samples / (seq_max / 1e3), "unit": "iters/s",
+                            "note": "the same genomes one after another through pyr3_iterate "
+                                    "(autotuned kernel), device time"},
         "gpu_launches": args.steps * len(gs),
         "clocks": clk,
     }

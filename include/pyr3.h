@@ -81,15 +81,19 @@ typedef struct {
 /* Pool every distinct histogram bucket of a warp (__match_any_sync) instead
    of only the warp's hot bucket. */
 #define PYR3_ITER_AGGREGATE 2u
-/* Chaos kernel.  Without either flag an autotuner picks, per genome
- * structure, the faster of the two on the first launch of at least 2^26
- * samples (that launch then waits for its trial runs), and smaller launches
- * before that use the barrier kernel.  The barrier kernel runs each round of
- * a CTA's walkers in xform order between barriers; the queue kernel (genomes
- * of up to 32 xforms) keeps per-xform walker queues so warps run one xform
- * at a time without barriers. */
+/* Chaos kernel.  Without a kernel flag an autotuner picks, per genome
+ * structure, the fastest on the first launch of at least 2^26 samples (that
+ * launch then waits for its trial runs), and smaller launches before that
+ * use the barrier kernel.  The barrier kernel runs each round of a CTA's
+ * walkers in xform order between barriers; the queue kernel (genomes of up
+ * to 32 xforms) keeps per-xform walker queues so warps run one xform at a
+ * time without barriers; the wave kernel (genomes of up to 32 xforms) keeps
+ * every walker of the launch in device memory grouped by next xform and
+ * advances all of them one iteration per launch.  A kernel that cannot
+ * serve a genome or a request falls back to the barrier kernel. */
 #define PYR3_ITER_KERNEL_BARRIER 4u
 #define PYR3_ITER_KERNEL_QUEUE 8u
+#define PYR3_ITER_KERNEL_WAVE 16u
 
 /* present() request (src/renderer.ts:148-158, visualize.ts:178-204). */
 typedef struct {
@@ -182,6 +186,9 @@ int pyr3_info(pyr3_renderer *r, uint32_t *super_w, uint32_t *super_h, void **dev
 int pyr3_counters(pyr3_renderer *r, uint64_t *samples, uint64_t *splats);
 /* Device time in ms of the last pyr3_iterate chaos launch (CUDA events). */
 int pyr3_last_iterate_ms(pyr3_renderer *r, float *ms);
+/* Kernel launches the last pyr3_iterate issued (the wave kernel issues one
+ * per iteration; autotuner trials included). */
+int pyr3_last_iterate_launches(pyr3_renderer *r, uint64_t *launches);
 
 /* CUDA-event timing on the renderer's stream: record mark `slot` (0..7),
  * then read the device time between two marks (waits for the later one). */

@@ -26,6 +26,7 @@ ITER_EXACT_WALKERS = 1
 ITER_AGGREGATE = 2
 ITER_KERNEL_BARRIER = 4
 ITER_KERNEL_QUEUE = 8
+ITER_KERNEL_WAVE = 16
 
 
 class Pyr3Error(RuntimeError):
@@ -85,6 +86,7 @@ _SIGS = {
                             C.POINTER(C.c_void_p)]),
     "pyr3_counters": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "pyr3_last_iterate_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "pyr3_last_iterate_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "pyr3_mark": (C.c_int, [C.c_void_p, C.c_int32]),
     "pyr3_elapsed": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_float)]),
     "pyr3_flush_l2": (C.c_int, [C.c_void_p, C.c_uint64]),

@@ -74,6 +74,18 @@ struct ChaosArgs {
   uint32_t cta_slots;
 };
 
+// Host mirror of WaveArgs in csrc/jit/chaos_kernel.cuh (the wave kernel's
+// second argument block).
+struct WaveArgs {
+  uint32_t* st;
+  uint32_t* cnt;
+  uint64_t cap;
+  uint32_t mode;
+  uint32_t rd_buf, wr_buf;
+  uint32_t rd_cnt, wr_cnt, zero_cnt;
+};
+static_assert(sizeof(WaveArgs) == 48, "WaveArgs layout");
+
 // ---- host restatements of the reference's host-side math --------------
 // Pick table (src/genome.ts:482-534) as per-row boundaries: start[r][j] is
 // the first grain index whose table entry is >= j, so the device recovers
@@ -193,11 +205,14 @@ struct pyr3_renderer {
   uint64_t* d_counters = nullptr;
   uint64_t* d_sched = nullptr;  // queue kernel: [0] walkers handed out, [1] sticky fault flags
   uint32_t* d_wrec = nullptr;   // queue kernel: walker records (CTAs x slots)
+  uint32_t* d_wave = nullptr;   // wave kernel: walker state, then 3 x NXF region counts
+  size_t wave_bytes = 0;
   size_t wrec_cap = 0;
   bool capture = false;
   float last_ms = 0.0f;
+  uint64_t last_launches = 0;  // kernel launches of the last pyr3_iterate
   cudaEvent_t marks[8] = {};
-  cudaEvent_t tune[3] = {};  // kernel autotuner
+  cudaEvent_t tune[4] = {};  // kernel autotuner
   void* d_flush = nullptr;
   size_t flush_bytes = 0;
   std::vector<std::shared_ptr<pyr3::ChaosModule>> modules;  // keep-alive
@@ -312,6 +327,7 @@ PYR3_API int pyr3_destroy(pyr3_renderer* r) {
   cudaFree(r->d_counters);
   cudaFree(r->d_sched);
   cudaFree(r->d_wrec);
+  cudaFree(r->d_wave);
   cudaFree(r->d_flush);
   for (auto& e : r->marks)
     if (e) cudaEventDestroy(e);
@@ -426,12 +442,100 @@ int launch_chaos(pyr3_renderer* r, const pyr3::ChaosModule& m, bool queue, Chaos
     CUDA_TRY(cudaMemsetAsync(r->d_sched, 0, 8, r->stream));
     LAUNCH_TRY(m.queue, (unsigned)ctas, (unsigned)(pyr3::kQueueWarps * 32), m.queue_smem, r->stream,
                params);
+    r->last_launches += 1;
   } else {
     const unsigned grid = (unsigned)std::min<uint64_t>((nw + m.wpb - 1) / m.wpb, ctas);
     LAUNCH_TRY(m.chaos, grid, (unsigned)m.wpb, m.smem, r->stream, params);
+    r->last_launches += 1;
   }
   *used = nw;
   return PYR3_OK;
+}
+
+// Walkers of a wave launch of `total` samples: about 2,000 iterations each,
+// so the 200-iteration burn-in stays near 10 %, yet enough that every
+// launch fills the GPU twice over; at most 2^20, whose state (42 u32 per
+// walker and region, two buffers) stays within a few GB.
+constexpr uint64_t kWaveMaxWalkers = 1ull << 21;
+uint64_t wave_walkers(pyr3_renderer* r, const pyr3::ChaosModule& m, uint64_t total) {
+  const uint64_t fill =
+      (uint64_t)device_sms(r->device) * (uint64_t)m.wave_blocks_per_sm * pyr3::kWaveBlock * 2;
+  const uint64_t want = std::min<uint64_t>(1ull << 20, std::max<uint64_t>(fill, total / 2000));
+  return std::max<uint64_t>(1, std::min<uint64_t>(want, total));
+}
+
+// The wave kernel for `total` samples on walkers walker_base.. (`walkers`
+// of them, 0: wave_walkers): a seeding launch, one launch per iteration
+// (the iterations of the longest walker, fuse included), and a last launch
+// that finishes the walkers whose bad-value retries did not count as
+// iterations.
+int launch_wave(pyr3_renderer* r, const pyr3::ChaosModule& m, ChaosArgs A, uint64_t total,
+                uint64_t walker_base, uint64_t walkers, uint64_t* used) {
+  const uint64_t nw = walkers ? walkers : wave_walkers(r, m, total);
+  if (nw > kWaveMaxWalkers) return fail(PYR3_E_INVALID, "wave kernel: more than 2^21 walkers");
+  const uint64_t base = total / nw, extra = total % nw;
+  if (base + 1 + kFuse > 0xffffffffull)
+    return fail(PYR3_E_INVALID, "too many iterations per walker for one launch (> 2^32)");
+  A.walker_base = walker_base;
+  A.n_walkers = nw;
+  A.iters_base = base;
+  A.iters_extra = extra;
+  const uint64_t wb = pyr3::kWaveBlock;
+  const uint64_t cap = (nw + wb - 1) / wb * wb;
+  const size_t nxf = (size_t)m.nxf;
+  const size_t st_words = 2 * nxf * pyr3::kWaveFields * cap;
+  const size_t bytes = (st_words + 3 * nxf) * 4;
+  if (bytes > r->wave_bytes) {
+    CUDA_TRY(cudaStreamSynchronize(r->stream));
+    cudaFree(r->d_wave);
+    r->d_wave = nullptr;
+    r->wave_bytes = 0;
+    CUDA_TRY(cudaMalloc(&r->d_wave, bytes));
+    r->wave_bytes = bytes;
+  }
+  WaveArgs W;
+  std::memset(&W, 0, sizeof W);
+  W.st = r->d_wave;
+  W.cnt = r->d_wave + st_words;
+  W.cap = cap;
+  CUDA_TRY(cudaMemsetAsync(W.cnt, 0, 3 * nxf * 4, r->stream));
+  void* params[] = {&A, &W};
+  const unsigned seed_grid = (unsigned)((nw + wb - 1) / wb);
+  const unsigned grid = seed_grid + (unsigned)nxf;  // >= chunks of any split into regions
+  W.mode = 0;
+  W.rd_buf = 1;
+  W.wr_buf = 0;
+  W.rd_cnt = 2;
+  W.wr_cnt = 0;
+  W.zero_cnt = 1;
+  LAUNCH_TRY(m.wave, seed_grid, (unsigned)wb, m.wave_smem, r->stream, params);
+  r->last_launches += 1;
+  const uint64_t steps = base + (extra ? 1 : 0) + kFuse;
+  for (uint64_t s = 1; s <= steps + 1; ++s) {
+    W.mode = s <= steps ? 1u : 2u;
+    W.rd_buf = (uint32_t)((s - 1) & 1);
+    W.wr_buf = W.rd_buf ^ 1u;
+    W.rd_cnt = (uint32_t)((s - 1) % 3);
+    W.wr_cnt = (uint32_t)(s % 3);
+    W.zero_cnt = (uint32_t)((s + 1) % 3);
+    LAUNCH_TRY(m.wave, grid, (unsigned)wb, m.wave_smem, r->stream, params);
+    r->last_launches += 1;
+  }
+  *used = nw;
+  return PYR3_OK;
+}
+
+enum KernelKind { kBarrier = 0, kQueue = 1, kWave = 2 };
+
+// Walkers a launch of `total` samples uses on kernel `kind` by default.
+uint64_t kind_walkers(pyr3_renderer* r, const pyr3::ChaosModule& m, int kind, uint64_t total) {
+  return kind == kWave ? wave_walkers(r, m, total) : pool_walkers(r, m, kind == kQueue, total);
+}
+
+int launch_kind(pyr3_renderer* r, const pyr3::ChaosModule& m, int kind, const ChaosArgs& A,
+                uint64_t total, uint64_t walker_base, uint64_t walkers, uint64_t* used) {
+  if (kind == kWave) return launch_wave(r, m, A, total, walker_base, walkers, used);
+  return launch_chaos(r, m, kind == kQueue, A, total, walker_base, walkers, used);
 }
 }  // namespace
 
@@ -523,53 +627,72 @@ PYR3_API int pyr3_iterate(pyr3_renderer* r, const pyr3_genome* g, const pyr3_ite
 
   const bool exact = (o->flags & PYR3_ITER_EXACT_WALKERS) != 0;
   uint64_t done = 0, walker_base = 0, used = 0;
-  bool use_queue = false;
+  const bool wave_ok = m->wave && (!exact || o->walkers <= kWaveMaxWalkers);
+  int kind = kBarrier;
+  r->last_launches = 0;
   CUDA_TRY(cudaEventRecord(r->ev0, r->stream));
-  if (!m->queue || (o->flags & PYR3_ITER_KERNEL_BARRIER)) {
-    use_queue = false;
+  if (o->flags & PYR3_ITER_KERNEL_BARRIER) {
+    kind = kBarrier;
   } else if (o->flags & PYR3_ITER_KERNEL_QUEUE) {
-    use_queue = true;
+    kind = m->queue ? kQueue : kBarrier;
+  } else if (o->flags & PYR3_ITER_KERNEL_WAVE) {
+    kind = wave_ok ? kWave : kBarrier;
   } else if (m->choice.load() >= 0) {
-    use_queue = m->choice.load() == 1;
+    kind = m->choice.load();
+    if ((kind == kQueue && !m->queue) || (kind == kWave && !wave_ok)) kind = kBarrier;
   } else if (!exact && total >= kTuneMinSamples) {
     // Autotune: the first large launch of this genome structure runs a
     // short trial on each chaos kernel -- with the walker count that kernel
     // would use for the whole launch, so that the trial sees the same
     // occupancy and queue lengths -- and the rest of the samples (and every
     // later launch) on the kernel whose predicted time for the remaining
-    // samples, burn-in included, is lower.  Every sample still lands in the
+    // samples, burn-in included, is lowest.  Every sample still lands in the
     // histogram; each launch uses fresh walker indices.
-    const uint64_t nw_b = pool_walkers(r, *m, false, total), nw_q = pool_walkers(r, *m, true, total);
-    const uint64_t t_b = nw_b * std::max<uint64_t>(1, total / 32 / nw_b);
-    const uint64_t t_q = nw_q * std::max<uint64_t>(1, total / 32 / nw_q);
-    float ms_b = 0.0f, ms_q = 0.0f;
+    int cand[3];
+    int nc = 0;
+    cand[nc++] = kBarrier;
+    if (m->queue) cand[nc++] = kQueue;
+    if (m->wave) cand[nc++] = kWave;
+    uint64_t nw[3], tr[3];
+    float ms[3];
     CUDA_TRY(cudaEventRecord(r->tune[0], r->stream));
-    rc = launch_chaos(r, *m, false, A, t_b, 0, nw_b, &used);
-    if (rc) return rc;
-    walker_base += used;
-    CUDA_TRY(cudaEventRecord(r->tune[1], r->stream));
-    rc = launch_chaos(r, *m, true, A, t_q, walker_base, nw_q, &used);
-    if (rc) return rc;
-    walker_base += used;
-    CUDA_TRY(cudaEventRecord(r->tune[2], r->stream));
-    CUDA_TRY(cudaEventSynchronize(r->tune[2]));
-    CUDA_TRY(cudaEventElapsedTime(&ms_b, r->tune[0], r->tune[1]));
-    CUDA_TRY(cudaEventElapsedTime(&ms_q, r->tune[1], r->tune[2]));
-    done = t_b + t_q;
+    for (int c = 0; c < nc; ++c) {
+      nw[c] = kind_walkers(r, *m, cand[c], total);
+      tr[c] = nw[c] * std::max<uint64_t>(1, total / 32 / nw[c]);
+      rc = launch_kind(r, *m, cand[c], A, tr[c], walker_base, nw[c], &used);
+      if (rc) return rc;
+      walker_base += used;
+      done += tr[c];
+      CUDA_TRY(cudaEventRecord(r->tune[c + 1], r->stream));
+    }
+    CUDA_TRY(cudaEventSynchronize(r->tune[nc]));
     const double rest = (double)(total > done ? total - done : 0);
-    // ms per iteration (burn-in iterations included) times the iterations
-    // the rest of the launch needs on each kernel.
-    const double per_b = ms_b / ((double)t_b + (double)nw_b * kFuse);
-    const double per_q = ms_q / ((double)t_q + (double)nw_q * kFuse);
-    use_queue = per_q * (rest + (double)nw_q * kFuse) < per_b * (rest + (double)nw_b * kFuse);
-    m->choice.store(use_queue ? 1 : 0);
+    double best = 0.0;
+    for (int c = 0; c < nc; ++c) {
+      CUDA_TRY(cudaEventElapsedTime(&ms[c], r->tune[c], r->tune[c + 1]));
+      // ms per iteration (burn-in iterations included) times the
+      // iterations the rest of the launch needs on this kernel.
+      const double per = ms[c] / ((double)tr[c] + (double)nw[c] * kFuse);
+      const double pred = per * (rest + (double)kind_walkers(r, *m, cand[c], total) * kFuse);
+      if (c == 0 || pred < best) {
+        best = pred;
+        kind = cand[c];
+      }
+    }
+    m->choice.store(kind);
   }
   if (done < total) {
-    if (exact) rc = launch_chaos(r, *m, use_queue, A, total, 0, o->walkers, &used);
-    else rc = launch_chaos(r, *m, use_queue, A, total - done, walker_base, 0, &used);
+    if (exact) rc = launch_kind(r, *m, kind, A, total, 0, o->walkers, &used);
+    else rc = launch_kind(r, *m, kind, A, total - done, walker_base, 0, &used);
     if (rc) return rc;
   }
   CUDA_TRY(cudaEventRecord(r->ev1, r->stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_last_iterate_launches(pyr3_renderer* r, uint64_t* launches) {
+  if (!r || !launches) return fail(PYR3_E_INVALID, "null argument");
+  *launches = r->last_launches;
   return PYR3_OK;
 }
 
@@ -820,13 +943,14 @@ PYR3_API int pyr3_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t
 }
 
 namespace {
-// The queue chaos kernel sets sched[1] if one of its bounded waits ran out
-// (a scheduling fault); it stays set until the next reset.
+// The queue and wave chaos kernels set sched[1] if one of their bounded
+// waits ran out (a walker-queue wait, or a chunk copy that did not land);
+// it stays set until the next reset.
 int check_sched(pyr3_renderer* r) {
   uint64_t f = 0;
   CUDA_TRY(cudaMemcpyAsync(&f, r->d_sched + 1, 8, cudaMemcpyDeviceToHost, r->stream));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
-  if (f) return fail(PYR3_E_CUDA, "chaos kernel: a walker-queue wait exceeded its limit");
+  if (f) return fail(PYR3_E_CUDA, "chaos kernel: a bounded wait (walker queue or chunk copy) exceeded its limit");
   return PYR3_OK;
 }
 }  // namespace

@@ -169,6 +169,7 @@ std::string gen_chain(const XformShape& x, const std::string& base, const char* 
 }  // namespace
 
 bool use_queue(int nxf) { return nxf >= 1 && nxf <= kQueueMaxXforms; }
+bool use_wave(int nxf) { return nxf >= 1 && nxf <= kWaveMaxXforms; }
 
 namespace {
 
@@ -178,7 +179,8 @@ std::string gen_chaos_source(const GenomeShape& s, int wpb, bool aggregate) {
   o << "#define NXF " << nxf << "\n#define WPB " << wpb << "\n#define HAS_FINAL "
     << (s.has_final ? 1 : 0) << "\n#define FINAL_SLOT " << nxf << "\n#define PICK_LINEAR "
     << (nxf <= 16 ? 1 : 0) << "\n#define AGGREGATE " << (aggregate ? 1 : 0) << "\n#define QUEUE "
-    << (use_queue(nxf) ? 1 : 0) << "\n#define QWARPS " << kQueueWarps << "\n";
+    << (use_queue(nxf) ? 1 : 0) << "\n#define QWARPS " << kQueueWarps << "\n#define WAVE "
+    << (use_wave(nxf) ? 1 : 0) << "\n#define WAVE_MINB " << kWaveMinBlocks << "\n";
   o << library_source() << "\n";
   o << kSrcChaosPre << "\n";
   o << "VDEV void xform_chain(int k, float2 p, float pz, Ctx& c, ChainOut& o) {\n  switch (k) {\n";
@@ -331,6 +333,26 @@ int get_chaos_module(const GenomeShape& s, int wpb, bool aggregate,
                                                        m->queue_smem);
     if (cr == cudaSuccess && qb >= 1) m->queue_blocks_per_sm = qb;
     else m->queue = nullptr;  // not resident: the barrier kernel serves this structure
+  }
+  if (use_wave(nxf)) {
+    // Shared memory of the wave kernel (chaos_kernel.cuh, WAVE): palette,
+    // ISAAC state [36][WB], output staging [6][WB], sorted destinations,
+    // per-xform counts / offsets / bases, work item, sorted walker ids and
+    // keys, pick boundaries.
+    if (cudaLibraryGetKernel(&m->wave, m->mod, "chaos_wave_kernel") != cudaSuccess) {
+      *err = "chaos module is missing chaos_wave_kernel";
+      return PYR3_E_CUDA;
+    }
+    const size_t wb = kWaveBlock;
+    m->wave_smem = 256 * 16 + 36 * wb * 4 + 6 * wb * 4 + wb * 4 + (size_t)(3 * nxf + 1) * 4 + 3 * 4 +
+                   wb * 2 + wb + (size_t)(nxf + 1) * nxf * 2;
+    cudaFuncSetAttribute((const void*)m->wave, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)m->wave_smem);
+    int wbn = 0;
+    cr = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wbn, (const void*)m->wave, kWaveBlock,
+                                                       m->wave_smem);
+    if (cr == cudaSuccess && wbn >= 1) m->wave_blocks_per_sm = wbn;
+    else m->wave = nullptr;  // not resident: another kernel serves this structure
   }
   m->blocks_per_sm = nb;
   {

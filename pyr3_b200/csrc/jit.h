@@ -20,9 +20,18 @@ constexpr int kNumVariations = 326;
 constexpr int kQueueMaxXforms = 32;
 constexpr int kQueueWarps = 16;
 constexpr int kQueueSlots = 2048;
-constexpr int kQueueStageWords = 36 * 33 + 7 * 32;
+constexpr int kQueueStageWords = 44 * 33 + 32;
 constexpr int kWalkerRecordBytes = 192;
 bool use_queue(int nxf);
+// Wave chaos kernel (genomes of up to kWaveMaxXforms xforms): every walker
+// of a launch resident in global memory as kWaveFields u32 per walker,
+// grouped by next xform; one launch per iteration, kWaveBlock walkers per
+// block.
+constexpr int kWaveMaxXforms = 32;
+constexpr int kWaveBlock = 256;
+constexpr int kWaveFields = 42;
+constexpr int kWaveMinBlocks = 3;
+bool use_wave(int nxf);
 
 // The part of a genome that changes the generated code: how many xforms,
 // which variations each one sums (in slot order), which have a post
@@ -60,8 +69,12 @@ struct ChaosModule {
   cudaKernel_t queue = nullptr;
   size_t queue_smem = 0;
   int queue_blocks_per_sm = 0;
+  // chaos_wave_kernel (genomes of <= kWaveMaxXforms xforms), else null.
+  cudaKernel_t wave = nullptr;
+  size_t wave_smem = 0;
+  int wave_blocks_per_sm = 0;
   // Kernel choice of the autotuner for this structure: -1 not measured
-  // yet, 0 chaos_kernel, 1 chaos_queue_kernel.
+  // yet, 0 chaos_kernel, 1 chaos_queue_kernel, 2 chaos_wave_kernel.
   std::atomic<int> choice{-1};
   ~ChaosModule();
 };

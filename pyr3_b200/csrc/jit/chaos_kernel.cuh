@@ -364,6 +364,41 @@ VDEV float3 accept_step(const ChaosArgs& A, const float4* pal, const Rng& rng, i
   return make_float3(pv.x + jx, pv.y + jy, nz);
 }
 
+// One pass of the reference's iteration loop (chaos.wgsl:8330-8731) for a
+// walker whose picked xform is k: the chain, the bad-value reseed with its
+// retry count, and on acceptance the final xform, jitter and splat.  The
+// walker state (position p, colour z, iteration index i, last accepted
+// xform prev (-1: none), consecutive bad values) is updated in place.
+VDEV void walker_iter(const ChaosArgs& A, const unsigned short* pst, const float4* pal,
+                      const Rng& rng, int k, float2& p, float& z, u32& i, int& prev, u32& consec,
+                      u64* acc_samples, u64* acc_in) {
+  const float2 p_start = p;
+  ChainOut o;
+  run_chain(A, pst, k, p_start, z, rng, o);
+  float2 pv = o.pv;
+  const float nz = o.nz;
+  if (bad_point(pv)) {
+    const float bx = rand_11(rng);
+    const float by = rand_11(rng);
+    pv = f2(bx, by);
+    consec += 1u;
+  } else {
+    consec = 0u;
+  }
+  float3 np = make_float3(pv.x, pv.y, nz);
+  if (consec > 0u && consec < 5u) {
+    if (i == 0u) i = 1u;  // the reference's rollback stops at 0
+  } else {
+    if (consec >= 5u) consec = 0u;
+    prev = k;
+    np = accept_step(A, pal, rng, k, pv, nz, o.dc_hit, o.dc, p_start, i >= A.fuse, acc_samples,
+                     acc_in);
+    i += 1u;
+  }
+  p = f2(np.x, np.y);
+  z = np.z;
+}
+
 // --------------------------------------------------------------- kernel
 extern "C" __global__ void __launch_bounds__(WPB)
 chaos_kernel(const __grid_constant__ ChaosArgs A) {
@@ -583,6 +618,7 @@ chaos_kernel(const __grid_constant__ ChaosArgs A) {
 #define QFULL 0x8000u
 #define WR_WORDS 48            // record stride in u32 (192 B)
 #define WR_PARTS 11            // uint4 parts that carry data (words 0..43)
+#define QSTAGE (44 * SST + 32)  // staging words per warp: 44 rows of SST, then the lanes' slots
 #define SST 33                 // staging stride between ISAAC fields: conflict-free
 #define QSPIN_LIMIT (1u << 22)
 #define QIDLE_CYCLES 4000000000ll  // ~2 s at 1.97 GHz without work while walkers are live
@@ -617,7 +653,7 @@ VDEV bool q_take(unsigned short* ring_k, u32 pos, u32* s) {
 VDEV u32 vld(const u32* p) { return *(const volatile u32*)p; }
 
 // Staged walker of lane `lane`: ISAAC fields at sst[k * SST + lane]; record
-// words 36..41 at sf[(w - 36) * 32 + lane]: x, y, z bits, iteration index,
+// words 36..41 at sf[(w - 36) * SST + lane]: x, y, z bits, iteration index,
 // fuse + iterations, prev xform (low byte, 0xff = none) | bad count << 8.
 // Seed walker lw of the launch into it (src/isaac.ts:194-229) and draw its
 // start point (chaos.wgsl:8302-8305).
@@ -628,39 +664,33 @@ VDEV void q_seed(const ChaosArgs& A, u32* sst, u32* sf, u32 lane, u64 lw) {
   const float y0 = rand_11(r);
   const float z0 = rand01(r);
   sf[lane] = __float_as_uint(x0);
-  sf[32 + lane] = __float_as_uint(y0);
-  sf[64 + lane] = __float_as_uint(z0);
-  sf[96 + lane] = 0u;
-  sf[128 + lane] = (u32)(A.iters_base + (lw < A.iters_extra ? 1ull : 0ull) + A.fuse);
-  sf[160 + lane] = 0xffu;
+  sf[SST + lane] = __float_as_uint(y0);
+  sf[2 * SST + lane] = __float_as_uint(z0);
+  sf[3 * SST + lane] = 0u;
+  sf[4 * SST + lane] = (u32)(A.iters_base + (lw < A.iters_extra ? 1ull : 0ull) + A.fuse);
+  sf[5 * SST + lane] = 0xffu;
 }
-// Record <-> staging for the first n lanes' slots in ssl (coalesced).
-VDEV void q_load(const ChaosArgs& A, const u32* ssl, u32 n, u32 lane, u32* sst, u32* sf) {
+// Record <-> staging for the first n lanes' slots in ssl (coalesced): lane
+// q moves 16-byte part j = q % WR_PARTS of record r = q / WR_PARTS, whose
+// four words sit in staging rows 4j..4j+3 (rows 42 and 43 are padding).
+VDEV void q_load(const ChaosArgs& A, const u32* ssl, u32 n, u32 lane, u32* sst) {
   const u32* base = A.wrec + (u64)blockIdx.x * QP * WR_WORDS;
   for (u32 q = lane; q < n * WR_PARTS; q += 32u) {
-    const u32 r = q / WR_PARTS, j = q % WR_PARTS;
+    const u32 r = q / WR_PARTS, j = q - r * WR_PARTS;
     const uint4 v = __ldcg((const uint4*)(base + (u64)ssl[r] * WR_WORDS) + j);
-    const u32 w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const u32 wd = j * 4u + (u32)e;
-      if (wd < 36u) sst[wd * SST + r] = w[e];
-      else if (wd < 42u) sf[(wd - 36u) * 32u + r] = w[e];
-    }
+    u32* d = sst + j * (4u * SST) + r;
+    d[0] = v.x;
+    d[SST] = v.y;
+    d[2 * SST] = v.z;
+    d[3 * SST] = v.w;
   }
 }
-VDEV void q_store(const ChaosArgs& A, const u32* ssl, u32 n, u32 lane, const u32* sst,
-                  const u32* sf) {
+VDEV void q_store(const ChaosArgs& A, const u32* ssl, u32 n, u32 lane, const u32* sst) {
   u32* base = A.wrec + (u64)blockIdx.x * QP * WR_WORDS;
   for (u32 q = lane; q < n * WR_PARTS; q += 32u) {
-    const u32 r = q / WR_PARTS, j = q % WR_PARTS;
-    u32 w[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const u32 wd = j * 4u + (u32)e;
-      w[e] = wd < 36u ? sst[wd * SST + r] : (wd < 42u ? sf[(wd - 36u) * 32u + r] : 0u);
-    }
-    __stcg((uint4*)(base + (u64)ssl[r] * WR_WORDS) + j, make_uint4(w[0], w[1], w[2], w[3]));
+    const u32 r = q / WR_PARTS, j = q - r * WR_PARTS;
+    const u32* d = sst + j * (4u * SST) + r;
+    __stcg((uint4*)(base + (u64)ssl[r] * WR_WORDS) + j, make_uint4(d[0], d[SST], d[2 * SST], d[3 * SST]));
   }
 }
 
@@ -668,8 +698,8 @@ extern "C" __global__ void __launch_bounds__(QWARPS * 32, 1)
 chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   float4* pal = (float4*)smem;                                  // [256]
-  u32* stage = (u32*)(pal + 256);                               // [QWARPS][36*SST + 7*32]
-  unsigned short* ring = (unsigned short*)(stage + QWARPS * (36 * SST + 7 * 32));  // [NXF][QP]
+  u32* stage = (u32*)(pal + 256);                               // [QWARPS][QSTAGE]
+  unsigned short* ring = (unsigned short*)(stage + QWARPS * QSTAGE);  // [NXF][QP]
   unsigned short* pst = ring + NXF * QP;                        // pick boundaries
   u32* qhead = (u32*)(pst + ((MAXRANK * NXF + 1) & ~1));
   u32* qtail = qhead + NXF;
@@ -683,9 +713,9 @@ chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
   if (t < (u32)NXF) { qhead[t] = 0u; qtail[t] = 0u; }
   if (t == 0) { *live = 0; *aff = 0u; }
   __syncthreads();
-  u32* sst = stage + warp * (36 * SST + 7 * 32);
-  u32* sf = sst + 36 * SST;
-  u32* ssl = sf + 6 * 32;                                       // slot of each lane
+  u32* sst = stage + warp * QSTAGE;
+  u32* sf = sst + 36 * SST;                                     // record words 36.. (stride SST)
+  u32* ssl = sst + 44 * SST;                                    // slot of each lane
 
   // ---- fill the slots, 32 at a time per warp
   for (u32 b = warp * 32u; b < A.cta_slots; b += QWARPS * 32u) {
@@ -705,7 +735,7 @@ chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
     // Store every lane whose slot exists (a prefix of the warp); slots that
     // got no walker are never queued, so their records are never read.
     const u32 nb = A.cta_slots - b < 32u ? A.cta_slots - b : 32u;
-    q_store(A, ssl, nb, lane, sst, sf);
+    q_store(A, ssl, nb, lane, sst);
     __threadfence_block();
     __syncwarp();
     if (have) {
@@ -770,7 +800,7 @@ chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
     if (__any_sync(0xffffffffu, fault)) { fault = true; break; }
     __syncwarp();
     __threadfence_block();
-    q_load(A, ssl, n, lane, sst, sf);
+    q_load(A, ssl, n, lane, sst);
     __syncwarp();
 
     // ---- one iteration of each staged walker (the warp runs xform k)
@@ -778,41 +808,21 @@ chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
     u32 nfn = 0u;
     if (lane < n) {
       const Rng rng{sst + lane, SST};
-      const float2 p_start = f2(__uint_as_float(sf[lane]), __uint_as_float(sf[32 + lane]));
-      ChainOut o;
-      run_chain(A, pst, (int)k, p_start, __uint_as_float(sf[64 + lane]), rng, o);
-      float2 pv = o.pv;
-      const float nz = o.nz;
-      u32 i = sf[96 + lane];
-      const u32 pb = sf[160 + lane];
+      float2 p = f2(__uint_as_float(sf[lane]), __uint_as_float(sf[SST + lane]));
+      float z = __uint_as_float(sf[2 * SST + lane]);
+      u32 i = sf[3 * SST + lane];
+      const u32 pb = sf[5 * SST + lane];
       u32 consec = pb >> 8;
       int prev = (int)(pb & 0xffu);
       if (prev == 0xff) prev = -1;
-      if (bad_point(pv)) {
-        const float bx = rand_11(rng);
-        const float by = rand_11(rng);
-        pv = f2(bx, by);
-        consec += 1u;
-      } else {
-        consec = 0u;
-      }
-      float3 np = make_float3(pv.x, pv.y, nz);
-      if (consec > 0u && consec < 5u) {
-        if (i == 0u) i = 1u;  // the reference's rollback stops at 0
-      } else {
-        if (consec >= 5u) consec = 0u;
-        prev = (int)k;
-        np = accept_step(A, pal, rng, (int)k, pv, nz, o.dc_hit, o.dc, p_start, i >= A.fuse,
-                         &acc_samples, &acc_in);
-        i += 1u;
-      }
-      sf[lane] = __float_as_uint(np.x);
-      sf[32 + lane] = __float_as_uint(np.y);
-      sf[64 + lane] = __float_as_uint(np.z);
-      sf[96 + lane] = i;
-      sf[160 + lane] = ((u32)prev & 0xffu) | (consec << 8);
+      walker_iter(A, pst, pal, rng, (int)k, p, z, i, prev, consec, &acc_samples, &acc_in);
+      sf[lane] = __float_as_uint(p.x);
+      sf[SST + lane] = __float_as_uint(p.y);
+      sf[2 * SST + lane] = __float_as_uint(z);
+      sf[3 * SST + lane] = i;
+      sf[5 * SST + lane] = ((u32)prev & 0xffu) | (consec << 8);
       push = true;
-      if (i >= sf[128 + lane]) {  // finished: the next walker of the launch, or retire the slot
+      if (i >= sf[4 * SST + lane]) {  // finished: the next walker of the launch, or retire the slot
         const u64 lw = atomicAdd((unsigned long long*)&A.sched[0], 1ull);
         if (lw < A.n_walkers) {
           q_seed(A, sst, sf, lane, lw);
@@ -826,7 +836,7 @@ chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
     }
     __syncwarp();
     // ---- write the records back, then push the slots
-    q_store(A, ssl, n, lane, sst, sf);
+    q_store(A, ssl, n, lane, sst);
     __threadfence_block();
     __syncwarp();
     const u32 pm = __ballot_sync(0xffffffffu, push);
@@ -849,6 +859,243 @@ chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
   }
 }
 #endif  // QUEUE
+
+#ifndef WAVE
+#define WAVE 0
+#endif
+#if WAVE
+// --------------------------------------------------------- wave kernel
+// Bulk-synchronous alternative for large launches: every walker of the
+// launch is resident in global memory, grouped by the xform it runs next,
+// and each launch of chaos_wave_kernel advances every walker by one
+// iteration.  Block b takes the b-th chunk of WB walkers in region order
+// (xform 0's chunks first), so all of a block's walkers run one xform --
+// full warps on one xform's straight-line code -- and the blocks resident
+// on the GPU at any moment run one or two xforms, which keeps the
+// instruction working set small.  After the iteration each block counting-
+// sorts its walkers by their next xform in shared memory, reserves room in
+// the next buffer's regions with one atomicAdd per xform, and writes the
+// walkers out in sorted order (coalesced).  No block ever waits on another.
+//
+// State: st[2][NXF][WF][cap] u32 (two buffers, field-major so a chunk's
+// field is one contiguous 1 KB line) -- fields 0..35 the ISAAC state in the
+// Rng layout, then x, y, z bits, iteration index, iterations to run (fuse
+// included), last accepted xform (low byte, 0xff = none) | bad count << 8.
+// Walker counts per region: cnt[3][NXF]; a launch reads cnt[rd_cnt], adds
+// into cnt[wr_cnt] and zeroes cnt[zero_cnt] for the launch after next.
+// Modes: 0 seeds walkers [b*WB, b*WB + WB) and sorts them by first pick;
+// 1 runs one iteration; 2 (the last launch) runs each remaining walker to
+// its end in place -- walkers still running after the planned launches are
+// the ones whose bad-value retries did not count as iterations.
+#define WB 256
+#define WF 42
+
+struct WaveArgs {
+  u32* st;
+  u32* cnt;
+  u64 cap;        // walkers per region (>= walkers in the launch)
+  u32 mode;
+  u32 rd_buf, wr_buf;
+  u32 rd_cnt, wr_cnt, zero_cnt;
+};
+
+VDEV u32* wave_field(const WaveArgs& W, u32 buf, u32 k, u32 f) {
+  return W.st + (((u64)buf * NXF + k) * WF + f) * W.cap;
+}
+
+// Bulk asynchronous copies (cp.async.bulk, no multicast) of a chunk's
+// fields into shared memory, completing on one mbarrier.  Every source
+// and destination is 1 KB aligned and every size a multiple of 16 bytes.
+#define WAVE_WAIT_LIMIT (1u << 24)
+VDEV u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+VDEV void mbar_init(u64* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n"
+               "fence.mbarrier_init.release.cluster;\n" ::"r"(smem_u32(bar)) : "memory");
+}
+VDEV void mbar_expect_tx(u64* bar, u32 bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n"
+               ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+VDEV void bulk_g2s(void* dst, const void* src, u32 bytes, u64* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// Wait for phase 0 of the barrier; false if WAVE_WAIT_LIMIT polls pass.
+VDEV bool mbar_wait0(u64* bar) {
+  for (u32 it = 0; it < WAVE_WAIT_LIMIT; ++it) {
+    u32 done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(smem_u32(bar)) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+extern "C" __global__ void __launch_bounds__(WB, WAVE_MINB)
+chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ WaveArgs W) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float4* pal = (float4*)smem;                                  // [256]
+  u32* srng = (u32*)(pal + 256);                                // [36][WB]
+  u32* sfs = srng + 36 * WB;                                    // [6][WB] output staging
+  u32* sdst = sfs + 6 * WB;                                     // [WB] destination of sorted slot
+  u32* scnt = sdst + WB;                                        // [NXF] walkers per next xform
+  u32* soff = scnt + NXF;                                       // [NXF + 1] sorted offsets
+  u32* sbase = soff + NXF + 1;                                  // [NXF] region positions
+  u32* swork = sbase + NXF;                                     // [3] xform, chunk, region count
+  unsigned short* sperm = (unsigned short*)(swork + 3);         // [WB] walker of sorted slot
+  unsigned char* skey = (unsigned char*)(sperm + WB);           // [WB] its next xform
+  unsigned short* pst = (unsigned short*)(skey + WB);           // pick boundaries
+
+  __shared__ __align__(8) u64 wbar;
+
+  const u32 t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  if (W.mode == 0u)
+    for (u32 i = t; i < 256u; i += WB) pal[i] = ((const float4*)A.palette)[i];
+  else if (t == 0)
+    mbar_init(&wbar);
+  for (u32 i = t; i < (u32)(MAXRANK * NXF); i += WB) pst[i] = A.pick_start[i];
+  if (blockIdx.x == 0 && t < (u32)NXF && W.mode != 2u) W.cnt[W.zero_cnt * NXF + t] = 0u;
+  if (W.mode != 0u && warp == 0) {
+    // This block's work item: chunk c of region k, regions in xform order.
+    const u32 c = lane < (u32)NXF ? W.cnt[W.rd_cnt * NXF + lane] : 0u;
+    const u32 nb = (c + WB - 1u) / WB;
+    u32 incl = nb;
+#pragma unroll
+    for (u32 o = 1; o < 32u; o <<= 1) {
+      const u32 v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const u32 m = __ballot_sync(0xffffffffu, incl > blockIdx.x);
+    const u32 k = m ? (u32)(__ffs(m) - 1) : 0u;
+    const u32 first = __shfl_sync(0xffffffffu, incl - nb, k);
+    const u32 ck = __shfl_sync(0xffffffffu, c, k);
+    if (lane == 0) {
+      swork[0] = m ? k : 0xffffffffu;
+      swork[1] = blockIdx.x - first;
+      swork[2] = ck;
+    }
+  }
+  __syncthreads();
+  const Rng rng{srng + t, WB};
+  u64 acc_samples = 0, acc_in = 0;
+  bool alive = false;
+  u32 nfn = 0u;
+  float2 p = f2(0.0f, 0.0f);
+  float z = 0.0f;
+  u32 i = 0u, iters = 0u, consec = 0u;
+  int prev = -1;
+  if (W.mode == 0u) {
+    const u64 lw = (u64)blockIdx.x * WB + t;
+    if (lw < A.n_walkers) {
+      seed_walker(rng, A.seed, A.walker_base + lw);
+      const float x0 = rand_11(rng);
+      const float y0 = rand_11(rng);
+      z = rand01(rng);
+      p = f2(x0, y0);
+      iters = (u32)(A.iters_base + (lw < A.iters_extra ? 1ull : 0ull) + A.fuse);
+      nfn = pick_xform(pst, (u32)NXF, irand(rng) & 16383u);
+      alive = true;
+    }
+  } else {
+    const u32 k = swork[0];
+    if (k == 0xffffffffu) return;  // uniform: past the end of the work list
+    const u32 pos0 = swork[1] * WB, pos = pos0 + t;
+    // One thread moves the chunk (42 fields x 1 KB) and the palette into
+    // shared memory; the chunk may extend past the region's walkers, never
+    // past its capacity.
+    if (t == 0) {
+      mbar_expect_tx(&wbar, (u32)(WF * WB * 4 + 256 * 16));
+      for (u32 f = 0; f < 36u; ++f)
+        bulk_g2s(srng + f * WB, wave_field(W, W.rd_buf, k, f) + pos0, WB * 4, &wbar);
+      for (u32 f = 0; f < 6u; ++f)
+        bulk_g2s(sfs + f * WB, wave_field(W, W.rd_buf, k, 36 + f) + pos0, WB * 4, &wbar);
+      bulk_g2s(pal, A.palette, 256 * 16, &wbar);
+    }
+    if (!__syncthreads_and(mbar_wait0(&wbar))) {
+      // The copy did not land in time (the whole block agrees): report it,
+      // wait once more (bounded) so no copy is still writing this block's
+      // shared memory, and drop the chunk.
+      if (t == 0) atomicOr((unsigned long long*)&A.sched[1], 2ull);
+      mbar_wait0(&wbar);
+      return;
+    }
+    if (pos < swork[2]) {
+      p = f2(__uint_as_float(sfs[t]), __uint_as_float(sfs[WB + t]));
+      z = __uint_as_float(sfs[2 * WB + t]);
+      i = sfs[3 * WB + t];
+      iters = sfs[4 * WB + t];
+      const u32 pb = sfs[5 * WB + t];
+      consec = pb >> 8;
+      prev = (pb & 0xffu) == 0xffu ? -1 : (int)(pb & 0xffu);
+      // Mode 1: one iteration and the next pick; mode 2: to the walker's end.
+      u32 kk = k;
+      for (;;) {
+        walker_iter(A, pst, pal, rng, (int)kk, p, z, i, prev, consec, &acc_samples, &acc_in);
+        if (i >= iters) break;
+        kk = pick_xform(pst, prev >= 0 ? (u32)prev : (u32)NXF, irand(rng) & 16383u);
+        if (W.mode == 1u) {
+          nfn = kk;
+          alive = true;
+          break;
+        }
+      }
+    }
+  }
+  if (A.counters) {
+    const u32 ds = __reduce_add_sync(0xffffffffu, (u32)acc_samples);
+    const u32 di = __reduce_add_sync(0xffffffffu, (u32)acc_in);
+    if (lane == 0) {
+      if (ds) atomicAdd(&A.counters[0], (u64)ds);
+      if (di) atomicAdd(&A.counters[1], (u64)di);
+    }
+  }
+  if (W.mode == 2u) return;
+
+  // ---- sort by next xform, reserve region space, write out
+  if (t < (u32)NXF) scnt[t] = 0u;
+  __syncthreads();
+  u32 rank = 0u;
+  if (alive) {
+    rank = atomicAdd(&scnt[nfn], 1u);
+    sfs[t] = __float_as_uint(p.x);
+    sfs[WB + t] = __float_as_uint(p.y);
+    sfs[2 * WB + t] = __float_as_uint(z);
+    sfs[3 * WB + t] = i;
+    sfs[4 * WB + t] = iters;
+    sfs[5 * WB + t] = ((u32)prev & 0xffu) | (consec << 8);
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const u32 c = lane < (u32)NXF ? scnt[lane] : 0u;
+    u32 incl = c;
+#pragma unroll
+    for (u32 o = 1; o < 32u; o <<= 1) {
+      const u32 v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane < (u32)NXF) {
+      soff[lane] = incl - c;
+      sbase[lane] = c ? atomicAdd(&W.cnt[W.wr_cnt * NXF + lane], c) : 0u;
+    }
+    if (lane == 31u) soff[NXF] = incl;
+  }
+  __syncthreads();
+  if (alive) {
+    const u32 q = soff[nfn] + rank;
+    sperm[q] = (unsigned short)t;
+    skey[q] = (unsigned char)nfn;
+    sdst[q] = sbase[nfn] + rank;
+  }
+  __syncthreads();
+  if (t < soff[NXF]) {
+    const u32 src = sperm[t], kk = skey[t], g = sdst[t];
+#pragma unroll 4
+    for (u32 f = 0; f < 36u; ++f) __stcg(wave_field(W, W.wr_buf, kk, f) + g, srng[f * WB + src]);
+#pragma unroll
+    for (u32 f = 0; f < 6u; ++f) __stcg(wave_field(W, W.wr_buf, kk, 36 + f) + g, sfs[f * WB + src]);
+  }
+}
+#endif  // WAVE
 
 // ------------------------------------------------------- stage test kernels
 // Xform pick of an explicit draw stream (chaos.wgsl:8343-8348).

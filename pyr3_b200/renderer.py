@@ -76,6 +76,7 @@ class Renderer:
                                filter_radius or DEFAULT_FILTER_RADIUS, device)
         _lib.check(_lib.lib().pyr3_create(C.byref(self._opts), C.byref(self._h)))
         self._capture = False
+        self.launches = 0  # chaos-kernel launches issued by iterate() so far
 
     # ---- properties (src/renderer.ts:283-288)
     @property
@@ -118,7 +119,7 @@ class Renderer:
                 phase_strength: float = 1.0, phase_freq: float = 1.0, exact_walkers: bool = False,
                 aggregate: bool = False, kernel: str = "auto") -> None:
         """Accumulate walkers x iters samples (src/renderer.ts:227).
-        kernel: "auto" (the autotuner's choice), "barrier" or "queue"."""
+        kernel: "auto" (the autotuner's choice), "barrier", "queue" or "wave"."""
         gg = genome if isinstance(genome, GpuGenome) else GpuGenome(genome)
         trap = trap or {}
         modes = {"palette": 0, "flow": 1, "trap-distance": 2, "phase": 3}
@@ -130,8 +131,10 @@ class Renderer:
             trap.get("radius", 0.5), trap.get("angle", 0.0), trap.get("falloff", 2.0),
             trap.get("freq", 4.0), trap.get("strength", 1.0), phase_strength, phase_freq,
             (_lib.ITER_EXACT_WALKERS if exact_walkers else 0) | (_lib.ITER_AGGREGATE if aggregate else 0)
-            | {"auto": 0, "barrier": _lib.ITER_KERNEL_BARRIER, "queue": _lib.ITER_KERNEL_QUEUE}[kernel])
+            | {"auto": 0, "barrier": _lib.ITER_KERNEL_BARRIER, "queue": _lib.ITER_KERNEL_QUEUE,
+               "wave": _lib.ITER_KERNEL_WAVE}[kernel])
         _lib.check(_lib.lib().pyr3_iterate(self._h, C.byref(gg.c), C.byref(o)))
+        self.launches += self.last_iterate_launches()
 
     def present_opts(self, genome: Genome, force_de_off: bool = False,
                      transparent: bool = False) -> _lib.PresentOpts:
@@ -225,6 +228,11 @@ class Renderer:
         ms = C.c_float()
         _lib.check(_lib.lib().pyr3_last_iterate_ms(self._h, C.byref(ms)))
         return ms.value
+
+    def last_iterate_launches(self) -> int:
+        n = C.c_uint64()
+        _lib.check(_lib.lib().pyr3_last_iterate_launches(self._h, C.byref(n)))
+        return n.value
 
     def prepare(self, genome) -> None:
         gg = genome if isinstance(genome, GpuGenome) else GpuGenome(genome)

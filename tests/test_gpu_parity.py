@@ -317,7 +317,8 @@ def _collapse(hist, W, H, os_):
     return h.reshape(H, os_, W, os_, 4).sum(axis=(1, 3))
 
 
-@pytest.mark.parametrize("kind", ["c1_queue_kernel", "c1_barrier_kernel", "wide_barrier_kernel"])
+@pytest.mark.parametrize("kind", ["c1_queue_kernel", "c1_wave_kernel", "c1_barrier_kernel",
+                                  "wide_barrier_kernel"])
 def test_whole_render_statistical_parity(kind):
     """A genome on a 160x120 canvas: the CUDA renderer (its own walker pool)
     vs the reference's chaos_main on the CPU (1024 walkers), equal sample
@@ -338,7 +339,7 @@ def test_whole_render_statistical_parity(kind):
     r = R.create_renderer(W, H, 1)
     r.reset(g)
     r.iterate(g, seed=77, walkers=walkers, iters_per_walker=iters,
-              kernel="queue" if kind == "c1_queue_kernel" else "barrier")
+              kernel={"c1_queue_kernel": "queue", "c1_wave_kernel": "wave"}.get(kind, "barrier"))
     s, _ = r.counters()
     assert s == samples
     dev_hist, _, _ = r.read_histogram()
@@ -359,6 +360,70 @@ def test_whole_render_statistical_parity(kind):
     psnr = 10 * np.log10(1.0 / max(mse, 1e-20))
     print(f"log-density L1 {l1:.4%} (ref-vs-ref {floor:.4%})  PSNR {psnr:.2f} dB")
     assert psnr >= 40.0
+    r.destroy()
+
+
+def _linear_genome(n=12, seed=3, blowup=False):
+    """n xforms whose chains are affine maps only (linear variation, post
+    affines, a final xform), so every kernel computes the same bits; with
+    blowup one xform scales by 3e5, so walkers leave the 1e10 box and take
+    the bad-value retry path."""
+    rng = np.random.default_rng(seed)
+    lin = G.variation_index("linear")
+    xs = []
+    for k in range(n):
+        a, b, c, d, e, f = (float(v) for v in rng.uniform(-0.8, 0.8, 6))
+        xs.append(G.Xform(a=a, b=b, c=c, d=d, e=e, f=f, weight=float(rng.uniform(0.05, 1.0)),
+                          color=float(rng.uniform(0, 1)), color_speed=0.5,
+                          variations=[G.Variation(lin, float(rng.uniform(0.5, 1.0)))],
+                          post=tuple(float(v) for v in rng.uniform(-0.9, 0.9, 6)) if k % 3 == 0 else None))
+    if blowup:
+        xs[1].a, xs[1].b, xs[1].d, xs[1].e = 3e5, 0.0, 0.0, 3e5
+        xs[1].weight = 0.5
+    fin = G.Xform(a=0.9, b=0.1, c=0.05, d=-0.1, e=0.9, f=0.0, weight=0.0, color=0.3, color_speed=0.2,
+                  variations=[G.Variation(lin, 1.0)])
+    g = workloads.plain_small()
+    g.xforms, g.finalxform = xs, fin
+    g.scale = 320 / 4
+    return g
+
+
+@pytest.mark.parametrize("blowup", [False, True])
+def test_wave_and_queue_kernels_match_barrier_kernel_bit_exact(blowup):
+    """Exact walkers, affine-only chains: the wave kernel (walkers regrouped
+    by xform between launches, last launch draining retried walkers) and the
+    queue kernel give the barrier kernel's histogram bit for bit, with the
+    same sample and in-canvas counts."""
+    g = _linear_genome(blowup=blowup)
+    res = {}
+    for kern in ("barrier", "wave", "queue"):
+        r = R.create_renderer(320, 240, 1)
+        r.reset(g)
+        r.iterate(g, seed=9, walkers=20_000, iters_per_walker=300, exact_walkers=True, kernel=kern)
+        s, n_in = r.counters()
+        h, _, _ = r.read_histogram()
+        res[kern] = (s, n_in, h)
+        r.destroy()
+    s0, n0, h0 = res["barrier"]
+    assert s0 == 20_000 * 300 and n0 > 0
+    for kern in ("wave", "queue"):
+        s, n_in, h = res[kern]
+        assert (s, n_in) == (s0, n0), kern
+        assert np.array_equal(h, h0), kern
+
+
+def test_wave_kernel_pool_split():
+    """Default (pooled) walkers on the wave kernel with a sample total that
+    does not divide evenly: every sample is counted once and the count
+    channel holds 255 per in-canvas splat."""
+    g = _linear_genome(n=5, seed=11, blowup=True)
+    r = R.create_renderer(320, 240, 1)
+    r.reset(g)
+    r.iterate(g, seed=2, walkers=777, iters_per_walker=13_001, kernel="wave")
+    s, n_in = r.counters()
+    assert s == 777 * 13_001
+    hist, _, _ = r.read_histogram()
+    assert int(hist.reshape(-1, 4)[:, 3].astype(np.uint64).sum()) == 255 * n_in
     r.destroy()
 
 
