@@ -336,7 +336,7 @@ int get_chaos_module(const GenomeShape& s, int wpb, bool aggregate,
   }
   if (use_wave(nxf)) {
     // Shared memory of the wave kernel (chaos_kernel.cuh, WAVE): palette,
-    // ISAAC state [36][WB], output staging [6][WB], sorted destinations,
+    // ISAAC state + stash [43][WB], walker fields [6][WB], sorted destinations,
     // per-xform counts / offsets / bases, work item, sorted walker ids and
     // keys, pick boundaries.
     if (cudaLibraryGetKernel(&m->wave, m->mod, "chaos_wave_kernel") != cudaSuccess) {
@@ -344,7 +344,7 @@ int get_chaos_module(const GenomeShape& s, int wpb, bool aggregate,
       return PYR3_E_CUDA;
     }
     const size_t wb = kWaveBlock;
-    m->wave_smem = 256 * 16 + 36 * wb * 4 + 6 * wb * 4 + wb * 4 + (size_t)(3 * nxf + 1) * 4 + 3 * 4 +
+    m->wave_smem = 256 * 16 + 43 * wb * 4 + 6 * wb * 4 + wb * 4 + (size_t)(3 * nxf + 1) * 4 + 3 * 4 +
                    wb * 2 + wb + (size_t)(nxf + 1) * nxf * 2;
     cudaFuncSetAttribute((const void*)m->wave, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)m->wave_smem);

@@ -29,7 +29,7 @@ bool use_queue(int nxf);
 // block.
 constexpr int kWaveMaxXforms = 32;
 constexpr int kWaveBlock = 256;
-constexpr int kWaveFields = 42;
+constexpr int kWaveFields = 49;
 constexpr int kWaveMinBlocks = 3;
 bool use_wave(int nxf);
 

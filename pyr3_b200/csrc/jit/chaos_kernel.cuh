@@ -878,9 +878,17 @@ chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
 // walkers out in sorted order (coalesced).  No block ever waits on another.
 //
 // State: st[2][NXF][WF][cap] u32 (two buffers, field-major so a chunk's
-// field is one contiguous 1 KB line) -- fields 0..35 the ISAAC state in the
-// Rng layout, then x, y, z bits, iteration index, iterations to run (fuse
-// included), last accepted xform (low byte, 0xff = none) | bad count << 8.
+// field is one contiguous 1 KB line) -- fields 0..42 the ISAAC state in the
+// Rng layout with the early-refill stash, then x, y, z bits, iteration
+// index, iterations to run (fuse included), last accepted xform (low byte,
+// 0xff = none) | bad count << 8.
+//
+// ISAAC rounds: a walker needs one per 16 draws, and a draw site where any
+// lane of a warp runs dry makes the whole warp wait for that lane's round.
+// Each iteration therefore starts with isaac_early_refill: walkers with
+// fewer than 8 unread results move them to the stash and run the round
+// there, together, so a warp runs one round per iteration instead of one
+// per draw site.  The stream of values is unchanged.
 // Walker counts per region: cnt[3][NXF]; a launch reads cnt[rd_cnt], adds
 // into cnt[wr_cnt] and zeroes cnt[zero_cnt] for the launch after next.
 // Modes: 0 seeds walkers [b*WB, b*WB + WB) and sorts them by first pick;
@@ -888,7 +896,8 @@ chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
 // its end in place -- walkers still running after the planned launches are
 // the ones whose bad-value retries did not count as iterations.
 #define WB 256
-#define WF 42
+#define WF 49                  // state words per walker
+#define WRNG 43                // of which ISAAC state + stash (shared-memory rows)
 
 struct WaveArgs {
   u32* st;
@@ -898,6 +907,20 @@ struct WaveArgs {
   u32 rd_buf, wr_buf;
   u32 rd_cnt, wr_cnt, zero_cnt;
 };
+
+// Refill a walker's ISAAC block before it runs dry: with fewer than 8
+// results unread (and no stash in use) stash them, run the round, and mark
+// the new block full (cnt 16).
+VDEV void isaac_early_refill(const Rng& r) {
+  const u32 c = r.f(0);
+  if (c < 8u) {
+#pragma unroll
+    for (u32 j = 0; j < 7u; ++j)
+      if (j < c) r.f(36 + j) = r.f(20 + j);
+    isaac_round(r);
+    r.f(0) = (c << 8) | 16u;
+  }
+}
 
 VDEV u32* wave_field(const WaveArgs& W, u32 buf, u32 k, u32 f) {
   return W.st + (((u64)buf * NXF + k) * WF + f) * W.cap;
@@ -935,8 +958,8 @@ extern "C" __global__ void __launch_bounds__(WB, WAVE_MINB)
 chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ WaveArgs W) {
   extern __shared__ __align__(16) unsigned char smem[];
   float4* pal = (float4*)smem;                                  // [256]
-  u32* srng = (u32*)(pal + 256);                                // [36][WB]
-  u32* sfs = srng + 36 * WB;                                    // [6][WB] output staging
+  u32* srng = (u32*)(pal + 256);                                // [WRNG][WB]
+  u32* sfs = srng + WRNG * WB;                                  // [6][WB] walker fields
   u32* sdst = sfs + 6 * WB;                                     // [WB] destination of sorted slot
   u32* scnt = sdst + WB;                                        // [NXF] walkers per next xform
   u32* soff = scnt + NXF;                                       // [NXF + 1] sorted offsets
@@ -1000,15 +1023,15 @@ chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ W
     const u32 k = swork[0];
     if (k == 0xffffffffu) return;  // uniform: past the end of the work list
     const u32 pos0 = swork[1] * WB, pos = pos0 + t;
-    // One thread moves the chunk (42 fields x 1 KB) and the palette into
+    // One thread moves the chunk (WF fields x 1 KB) and the palette into
     // shared memory; the chunk may extend past the region's walkers, never
     // past its capacity.
     if (t == 0) {
       mbar_expect_tx(&wbar, (u32)(WF * WB * 4 + 256 * 16));
-      for (u32 f = 0; f < 36u; ++f)
+      for (u32 f = 0; f < (u32)WRNG; ++f)
         bulk_g2s(srng + f * WB, wave_field(W, W.rd_buf, k, f) + pos0, WB * 4, &wbar);
       for (u32 f = 0; f < 6u; ++f)
-        bulk_g2s(sfs + f * WB, wave_field(W, W.rd_buf, k, 36 + f) + pos0, WB * 4, &wbar);
+        bulk_g2s(sfs + f * WB, wave_field(W, W.rd_buf, k, WRNG + f) + pos0, WB * 4, &wbar);
       bulk_g2s(pal, A.palette, 256 * 16, &wbar);
     }
     if (!__syncthreads_and(mbar_wait0(&wbar))) {
@@ -1030,6 +1053,7 @@ chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ W
       // Mode 1: one iteration and the next pick; mode 2: to the walker's end.
       u32 kk = k;
       for (;;) {
+        isaac_early_refill(rng);
         walker_iter(A, pst, pal, rng, (int)kk, p, z, i, prev, consec, &acc_samples, &acc_in);
         if (i >= iters) break;
         kk = pick_xform(pst, prev >= 0 ? (u32)prev : (u32)NXF, irand(rng) & 16383u);
@@ -1090,9 +1114,10 @@ chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ W
   if (t < soff[NXF]) {
     const u32 src = sperm[t], kk = skey[t], g = sdst[t];
 #pragma unroll 4
-    for (u32 f = 0; f < 36u; ++f) __stcg(wave_field(W, W.wr_buf, kk, f) + g, srng[f * WB + src]);
+    for (u32 f = 0; f < (u32)WRNG; ++f)
+      __stcg(wave_field(W, W.wr_buf, kk, f) + g, srng[f * WB + src]);
 #pragma unroll
-    for (u32 f = 0; f < 6u; ++f) __stcg(wave_field(W, W.wr_buf, kk, 36 + f) + g, sfs[f * WB + src]);
+    for (u32 f = 0; f < 6u; ++f) __stcg(wave_field(W, W.wr_buf, kk, WRNG + f) + g, sfs[f * WB + src]);
   }
 }
 #endif  // WAVE

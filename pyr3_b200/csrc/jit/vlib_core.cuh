@@ -159,6 +159,9 @@ VDEV float2 polar2(float r, float ang) {  // (r cos a, r sin a) with safe trig
 // One ISAAC stream per walker, held in shared memory as a [36][W] array of
 // u32 so that a warp touching 32 consecutive walkers hits 32 banks whatever
 // field it reads: field 0 = cnt, 1..3 = a, b, c, 4..19 = mem, 20..35 = rsl.
+// The wave kernel refills early (isaac_early_refill): it then keeps the
+// unread results of the old block in fields 36..42 and their count in bits
+// 8..15 of field 0, and irand serves those first.
 struct Rng {
   u32* s;  // &state[0][walker]
   u32 W;   // walkers per block (stride between fields)
@@ -197,6 +200,11 @@ VDEV void isaac_round(const Rng& r) { isaac_round_at(r.s, r.W); }
 
 VDEV u32 irand(const Rng& r) {
   u32 cnt = r.f(0);
+  if (cnt >= 256u) {  // results stashed by an early refill come first
+    const u32 sc = (cnt >> 8) - 1u;
+    r.f(0) = (sc << 8) | (cnt & 0xffu);
+    return r.f(36 + sc);
+  }
   if (cnt == 0u) {
     isaac_round(r);
     cnt = 15u;
