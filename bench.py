@@ -219,10 +219,11 @@ def bench_ours(args, ws, rank, local, dist):
         if g_close is None:
             _lib.check(lib.pyr3_reset(h, _lib.ptr(pal)))
             _lib.check(lib.pyr3_mark(h, 4))
-            r.iterate(gg, seed, walkers, iters)
+            r.iterate(gg, seed, walkers, iters, kernel=args.kernel)
         else:  # one motion-blurred frame: 8 sub-frames into one histogram
             _lib.check(lib.pyr3_mark(h, 4))
-            n, _ = animate.render_motion_frame(r, g, g_close, 0.5, ntemporal=8, seed=seed)
+            n, _ = animate.render_motion_frame(r, g, g_close, 0.5, ntemporal=8, seed=seed,
+                                               kernel=args.kernel)
             assert n == samples
         _lib.check(lib.pyr3_mark(h, 5))
         _lib.check(lib.pyr3_present_device(h, C.byref(p), samples, C.c_void_p(out_dev.data_ptr()),
@@ -256,9 +257,9 @@ def bench_ours(args, ws, rank, local, dist):
     def step_public(seed):
         if g_close is None:
             r.reset(g)
-            r.iterate(g, seed, walkers, iters)
+            r.iterate(g, seed, walkers, iters, kernel=args.kernel)
         else:
-            animate.render_motion_frame(r, g, g_close, 0.5, ntemporal=8, seed=seed)
+            animate.render_motion_frame(r, g, g_close, 0.5, ntemporal=8, seed=seed, kernel=args.kernel)
         r.present(g, samples, out=host_img)
 
     for k in range(max(1, args.warmup // 2)):
@@ -301,7 +302,8 @@ def bench_ours(args, ws, rank, local, dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded genome, pyr3_b200/workloads.py)",
-        "config": {"workload": args.config, "canvas": [W, H], "oversample": os_,
+        "config": {"workload": args.config, "chaos_kernel": args.kernel, "canvas": [W, H],
+                   "oversample": os_,
                    "quality_spp": g.quality, "samples_per_step": samples,
                    "xforms": len(g.xforms), "final_xform": g.finalxform is not None,
                    "density_estimation": g.density is not None,
@@ -443,6 +445,8 @@ def main():
     ap.add_argument("--config", default="headline", choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "barrier", "queue", "wave"],
+                    help="chaos kernel (auto: the autotuner's choice)")
     ap.add_argument("--samples", type=int, default=0,
                     help="override samples per step (small profiling case; not a bench number)")
     args = ap.parse_args()

@@ -205,8 +205,10 @@ struct pyr3_renderer {
   uint64_t* d_counters = nullptr;
   uint64_t* d_sched = nullptr;  // queue kernel: [0] walkers handed out, [1] sticky fault flags
   uint32_t* d_wrec = nullptr;   // queue kernel: walker records (CTAs x slots)
-  uint32_t* d_wave = nullptr;   // wave kernel: walker state, then 3 x NXF region counts
+  uint32_t* d_wave = nullptr;   // wave kernel: per population walker state + region counts
   size_t wave_bytes = 0;
+  cudaStream_t wave_aux = nullptr;  // wave kernel: the second population's stream
+  cudaEvent_t wave_fork = nullptr, wave_join = nullptr;
   size_t wrec_cap = 0;
   bool capture = false;
   float last_ms = 0.0f;
@@ -335,6 +337,9 @@ PYR3_API int pyr3_destroy(pyr3_renderer* r) {
     if (e) cudaEventDestroy(e);
   if (r->ev0) cudaEventDestroy(r->ev0);
   if (r->ev1) cudaEventDestroy(r->ev1);
+  if (r->wave_fork) cudaEventDestroy(r->wave_fork);
+  if (r->wave_join) cudaEventDestroy(r->wave_join);
+  if (r->wave_aux) cudaStreamDestroy(r->wave_aux);
   if (r->stream) cudaStreamDestroy(r->stream);
   delete r;
   return PYR3_OK;
@@ -408,6 +413,21 @@ uint64_t pool_walkers(pyr3_renderer* r, const pyr3::ChaosModule& m, bool queue, 
   return std::max<uint64_t>(1, std::min<uint64_t>(ctas * per_cta, std::min<uint64_t>(want, total)));
 }
 
+// The queue kernel's walker records (one slot set per resident CTA).
+int queue_reserve(pyr3_renderer* r, const pyr3::ChaosModule& m) {
+  const size_t rec_bytes = (size_t)m.queue_blocks_per_sm * device_sms(r->device) *
+                           pyr3::kQueueSlots * pyr3::kWalkerRecordBytes;
+  if (rec_bytes > r->wrec_cap) {
+    CUDA_TRY(cudaStreamSynchronize(r->stream));
+    cudaFree(r->d_wrec);
+    r->d_wrec = nullptr;
+    r->wrec_cap = 0;
+    CUDA_TRY(cudaMalloc(&r->d_wrec, rec_bytes));
+    r->wrec_cap = rec_bytes;
+  }
+  return PYR3_OK;
+}
+
 int launch_chaos(pyr3_renderer* r, const pyr3::ChaosModule& m, bool queue, ChaosArgs A,
                  uint64_t total, uint64_t walker_base, uint64_t walkers, uint64_t* used) {
   const int sms = device_sms(r->device);
@@ -426,15 +446,8 @@ int launch_chaos(pyr3_renderer* r, const pyr3::ChaosModule& m, bool queue, Chaos
     // One persistent CTA per SM; each fills cta_slots of its slots first
     // (fewer than all for small launches, so the walkers spread over every
     // SM) and refills slots from sched[0] as walkers finish.
-    const size_t rec_bytes = (size_t)ctas * per_cta * pyr3::kWalkerRecordBytes;
-    if (rec_bytes > r->wrec_cap) {
-      CUDA_TRY(cudaStreamSynchronize(r->stream));
-      cudaFree(r->d_wrec);
-      r->d_wrec = nullptr;
-      r->wrec_cap = 0;
-      CUDA_TRY(cudaMalloc(&r->d_wrec, rec_bytes));
-      r->wrec_cap = rec_bytes;
-    }
+    const int rc = queue_reserve(r, m);
+    if (rc) return rc;
     uint64_t slots = (nw + ctas - 1) / ctas;
     slots = std::min<uint64_t>(per_cta, (slots + 31) & ~31ull);
     A.wrec = r->d_wrec;
@@ -465,26 +478,40 @@ uint64_t wave_walkers(pyr3_renderer* r, const pyr3::ChaosModule& m, uint64_t tot
 }
 
 // The wave kernel for `total` samples on walkers walker_base.. (`walkers`
-// of them, 0: wave_walkers): a seeding launch, one launch per iteration
-// (the iterations of the longest walker, fuse included), and a last launch
-// that finishes the walkers whose bad-value retries did not count as
-// iterations.
-int launch_wave(pyr3_renderer* r, const pyr3::ChaosModule& m, ChaosArgs A, uint64_t total,
-                uint64_t walker_base, uint64_t walkers, uint64_t* used) {
-  const uint64_t nw = walkers ? walkers : wave_walkers(r, m, total);
+// of them, 0: wave_walkers).  The walkers are split into two populations,
+// each with its own state and launch sequence on its own stream: a seeding
+// launch, one launch per iteration (the iterations of its longest walker,
+// fuse included), and a last launch that finishes the walkers whose
+// bad-value retries did not count as iterations.  The two sequences
+// interleave, so one population's blocks fill the SMs while the other's
+// launch drains its last blocks (and across the gap between launches).
+// The walkers, their streams and iteration counts are those of one
+// population of `walkers`, so the histogram is the same.
+constexpr int kWavePops = 2;
+struct WavePlan {
+  int pops = 1;
+  uint64_t first[kWavePops] = {}, n[kWavePops] = {}, cap[kWavePops] = {};
+  size_t off[kWavePops] = {};  // u32 offset of each population's block in d_wave
+};
+
+// Split nw walkers into populations and make sure the state buffer and the
+// second stream exist.  Each population's block (two state buffers, then
+// its 3 x NXF counts) starts on a 256-byte boundary, so every chunk field
+// the bulk copies read is 1 KB aligned.
+int wave_reserve(pyr3_renderer* r, const pyr3::ChaosModule& m, uint64_t nw, WavePlan* plan) {
   if (nw > kWaveMaxWalkers) return fail(PYR3_E_INVALID, "wave kernel: more than 2^21 walkers");
-  const uint64_t base = total / nw, extra = total % nw;
-  if (base + 1 + kFuse > 0xffffffffull)
-    return fail(PYR3_E_INVALID, "too many iterations per walker for one launch (> 2^32)");
-  A.walker_base = walker_base;
-  A.n_walkers = nw;
-  A.iters_base = base;
-  A.iters_extra = extra;
   const uint64_t wb = pyr3::kWaveBlock;
-  const uint64_t cap = (nw + wb - 1) / wb * wb;
   const size_t nxf = (size_t)m.nxf;
-  const size_t st_words = 2 * nxf * pyr3::kWaveFields * cap;
-  const size_t bytes = (st_words + 3 * nxf) * 4;
+  plan->pops = nw >= 2 * wb ? kWavePops : 1;
+  size_t bytes = 0;
+  for (int p = 0; p < plan->pops; ++p) {
+    plan->first[p] = p == 0 ? 0 : plan->first[p - 1] + plan->n[p - 1];
+    plan->n[p] = p + 1 == plan->pops ? nw - plan->first[p] : (nw / plan->pops + wb - 1) / wb * wb;
+    plan->cap[p] = (plan->n[p] + wb - 1) / wb * wb;
+    plan->off[p] = bytes / 4;
+    const size_t blk = (2 * nxf * pyr3::kWaveFields * plan->cap[p] + 3 * nxf) * 4;
+    bytes += (blk + 255) / 256 * 256;
+  }
   if (bytes > r->wave_bytes) {
     CUDA_TRY(cudaStreamSynchronize(r->stream));
     cudaFree(r->d_wave);
@@ -493,33 +520,78 @@ int launch_wave(pyr3_renderer* r, const pyr3::ChaosModule& m, ChaosArgs A, uint6
     CUDA_TRY(cudaMalloc(&r->d_wave, bytes));
     r->wave_bytes = bytes;
   }
-  WaveArgs W;
-  std::memset(&W, 0, sizeof W);
-  W.st = r->d_wave;
-  W.cnt = r->d_wave + st_words;
-  W.cap = cap;
-  CUDA_TRY(cudaMemsetAsync(W.cnt, 0, 3 * nxf * 4, r->stream));
-  void* params[] = {&A, &W};
-  const unsigned seed_grid = (unsigned)((nw + wb - 1) / wb);
-  const unsigned grid = seed_grid + (unsigned)nxf;  // >= chunks of any split into regions
-  W.mode = 0;
-  W.rd_buf = 1;
-  W.wr_buf = 0;
-  W.rd_cnt = 2;
-  W.wr_cnt = 0;
-  W.zero_cnt = 1;
-  LAUNCH_TRY(m.wave, seed_grid, (unsigned)wb, m.wave_smem, r->stream, params);
-  r->last_launches += 1;
-  const uint64_t steps = base + (extra ? 1 : 0) + kFuse;
-  for (uint64_t s = 1; s <= steps + 1; ++s) {
-    W.mode = s <= steps ? 1u : 2u;
-    W.rd_buf = (uint32_t)((s - 1) & 1);
-    W.wr_buf = W.rd_buf ^ 1u;
-    W.rd_cnt = (uint32_t)((s - 1) % 3);
-    W.wr_cnt = (uint32_t)(s % 3);
-    W.zero_cnt = (uint32_t)((s + 1) % 3);
-    LAUNCH_TRY(m.wave, grid, (unsigned)wb, m.wave_smem, r->stream, params);
+  if (plan->pops > 1 && !r->wave_aux) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&r->wave_aux, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&r->wave_fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&r->wave_join, cudaEventDisableTiming));
+  }
+  return PYR3_OK;
+}
+
+int launch_wave(pyr3_renderer* r, const pyr3::ChaosModule& m, const ChaosArgs& A0, uint64_t total,
+                uint64_t walker_base, uint64_t walkers, uint64_t* used) {
+  const uint64_t nw = walkers ? walkers : wave_walkers(r, m, total);
+  const uint64_t base = total / nw, extra = total % nw;
+  if (base + 1 + kFuse > 0xffffffffull)
+    return fail(PYR3_E_INVALID, "too many iterations per walker for one launch (> 2^32)");
+  const uint64_t wb = pyr3::kWaveBlock;
+  const size_t nxf = (size_t)m.nxf;
+  WavePlan plan;
+  int rc = wave_reserve(r, m, nw, &plan);
+  if (rc) return rc;
+  const int pops = plan.pops;
+  cudaStream_t st[kWavePops] = {r->stream, r->wave_aux};
+  if (pops > 1) {
+    CUDA_TRY(cudaEventRecord(r->wave_fork, r->stream));
+    CUDA_TRY(cudaStreamWaitEvent(r->wave_aux, r->wave_fork, 0));
+  }
+  ChaosArgs A[kWavePops];
+  WaveArgs W[kWavePops];
+  uint64_t steps[kWavePops] = {}, max_steps = 0;
+  unsigned grid[kWavePops] = {};
+  for (int p = 0; p < pops; ++p) {
+    A[p] = A0;
+    A[p].walker_base = walker_base + plan.first[p];
+    A[p].n_walkers = plan.n[p];
+    A[p].iters_base = base;
+    A[p].iters_extra =
+        extra > plan.first[p] ? std::min<uint64_t>(extra - plan.first[p], plan.n[p]) : 0;
+    std::memset(&W[p], 0, sizeof W[p]);
+    W[p].st = r->d_wave + plan.off[p];
+    W[p].cnt = W[p].st + 2 * nxf * pyr3::kWaveFields * plan.cap[p];
+    W[p].cap = plan.cap[p];
+    CUDA_TRY(cudaMemsetAsync(W[p].cnt, 0, 3 * nxf * 4, st[p]));
+    W[p].mode = 0;
+    W[p].rd_buf = 1;
+    W[p].wr_buf = 0;
+    W[p].rd_cnt = 2;
+    W[p].wr_cnt = 0;
+    W[p].zero_cnt = 1;
+    void* params[] = {&A[p], &W[p]};
+    const unsigned seed_grid = (unsigned)((plan.n[p] + wb - 1) / wb);
+    LAUNCH_TRY(m.wave, seed_grid, (unsigned)wb, m.wave_smem, st[p], params);
     r->last_launches += 1;
+    grid[p] = seed_grid + (unsigned)nxf;  // >= chunks of any split into regions
+    steps[p] = base + (A[p].iters_extra ? 1 : 0) + kFuse;
+    max_steps = std::max(max_steps, steps[p]);
+  }
+  for (uint64_t s = 1; s <= max_steps + 1; ++s) {
+    for (int p = 0; p < pops; ++p) {
+      if (s > steps[p] + 1) continue;
+      W[p].mode = s <= steps[p] ? 1u : 2u;
+      W[p].rd_buf = (uint32_t)((s - 1) & 1);
+      W[p].wr_buf = W[p].rd_buf ^ 1u;
+      W[p].rd_cnt = (uint32_t)((s - 1) % 3);
+      W[p].wr_cnt = (uint32_t)(s % 3);
+      W[p].zero_cnt = (uint32_t)((s + 1) % 3);
+      void* params[] = {&A[p], &W[p]};
+      LAUNCH_TRY(m.wave, grid[p], (unsigned)wb, m.wave_smem, st[p], params);
+      r->last_launches += 1;
+    }
+  }
+  if (pops > 1) {
+    CUDA_TRY(cudaEventRecord(r->wave_join, r->wave_aux));
+    CUDA_TRY(cudaStreamWaitEvent(r->stream, r->wave_join, 0));
   }
   *used = nw;
   return PYR3_OK;
@@ -655,9 +727,18 @@ PYR3_API int pyr3_iterate(pyr3_renderer* r, const pyr3_genome* g, const pyr3_ite
     if (m->wave) cand[nc++] = kWave;
     uint64_t nw[3], tr[3];
     float ms[3];
-    CUDA_TRY(cudaEventRecord(r->tune[0], r->stream));
+    // Buffers first, so no trial's time includes an allocation.
     for (int c = 0; c < nc; ++c) {
       nw[c] = kind_walkers(r, *m, cand[c], total);
+      if (cand[c] == kQueue) rc = queue_reserve(r, *m);
+      if (cand[c] == kWave) {
+        WavePlan plan;
+        rc = wave_reserve(r, *m, nw[c], &plan);
+      }
+      if (rc) return rc;
+    }
+    CUDA_TRY(cudaEventRecord(r->tune[0], r->stream));
+    for (int c = 0; c < nc; ++c) {
       tr[c] = nw[c] * std::max<uint64_t>(1, total / 32 / nw[c]);
       rc = launch_kind(r, *m, cand[c], A, tr[c], walker_base, nw[c], &used);
       if (rc) return rc;
@@ -944,13 +1025,14 @@ PYR3_API int pyr3_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t
 
 namespace {
 // The queue and wave chaos kernels set sched[1] if one of their bounded
-// waits ran out (a walker-queue wait, or a chunk copy that did not land);
-// it stays set until the next reset.
+// waits ran out (a walker-queue wait, or a chunk copy that did not land) or
+// a chunk copy was refused for a misaligned source; it stays set until the
+// next reset.
 int check_sched(pyr3_renderer* r) {
   uint64_t f = 0;
   CUDA_TRY(cudaMemcpyAsync(&f, r->d_sched + 1, 8, cudaMemcpyDeviceToHost, r->stream));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
-  if (f) return fail(PYR3_E_CUDA, "chaos kernel: a bounded wait (walker queue or chunk copy) exceeded its limit");
+  if (f) return fail(PYR3_E_CUDA, "chaos kernel: a bounded wait (walker queue or chunk copy) exceeded its limit, or a chunk copy was refused");
   return PYR3_OK;
 }
 }  // namespace

@@ -1025,15 +1025,27 @@ chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ W
     const u32 pos0 = swork[1] * WB, pos = pos0 + t;
     // One thread moves the chunk (WF fields x 1 KB) and the palette into
     // shared memory; the chunk may extend past the region's walkers, never
-    // past its capacity.
+    // past its capacity.  Bulk copies need 16-byte aligned sources: the host
+    // lays the state out so they are, and a layout that is not is reported
+    // (sched[1] bit 2), not copied.
     if (t == 0) {
-      mbar_expect_tx(&wbar, (u32)(WF * WB * 4 + 256 * 16));
-      for (u32 f = 0; f < (u32)WRNG; ++f)
-        bulk_g2s(srng + f * WB, wave_field(W, W.rd_buf, k, f) + pos0, WB * 4, &wbar);
-      for (u32 f = 0; f < 6u; ++f)
-        bulk_g2s(sfs + f * WB, wave_field(W, W.rd_buf, k, WRNG + f) + pos0, WB * 4, &wbar);
-      bulk_g2s(pal, A.palette, 256 * 16, &wbar);
+      const bool aligned =
+          ((reinterpret_cast<unsigned long long>(wave_field(W, W.rd_buf, k, 0) + pos0) |
+            reinterpret_cast<unsigned long long>(A.palette) | (W.cap * 4ull)) & 15ull) == 0ull;
+      sbase[0] = aligned ? 1u : 0u;  // flag (sbase is free until the sort)
+      if (aligned) {
+        mbar_expect_tx(&wbar, (u32)(WF * WB * 4 + 256 * 16));
+        for (u32 f = 0; f < (u32)WRNG; ++f)
+          bulk_g2s(srng + f * WB, wave_field(W, W.rd_buf, k, f) + pos0, WB * 4, &wbar);
+        for (u32 f = 0; f < 6u; ++f)
+          bulk_g2s(sfs + f * WB, wave_field(W, W.rd_buf, k, WRNG + f) + pos0, WB * 4, &wbar);
+        bulk_g2s(pal, A.palette, 256 * 16, &wbar);
+      } else {
+        atomicOr((unsigned long long*)&A.sched[1], 4ull);
+      }
     }
+    __syncthreads();
+    if (sbase[0] == 0u) return;  // uniform: misaligned layout, nothing copied
     if (!__syncthreads_and(mbar_wait0(&wbar))) {
       // The copy did not land in time (the whole block agrees): report it,
       // wait once more (bounded) so no copy is still writing this block's
