@@ -793,6 +793,14 @@ PYR3_API int pyr3_last_iterate_ms(pyr3_renderer* r, float* ms) {
 // concurrently.  Walkers per genome are chosen for the batch: enough
 // iterations per walker to keep the 200-iteration burn-in under ~10 %,
 // since the GPU is filled by running many genomes at once.
+//
+// Genomes large enough to fill the GPU on their own (at least the
+// autotuner's 2^26 samples, pooled walkers) stay out of the graph: each
+// runs through pyr3_iterate on its autotuned kernel, one after another on
+// their renderers' streams, while the graph runs the small ones.  Their
+// genome records are copied at creation.  Graph genomes use module
+// instances 1.., so they never share a constant bank with pyr3_iterate's
+// instance 0.
 struct pyr3_batch {
   int device = 0;
   cudaStream_t origin = nullptr;
@@ -803,6 +811,12 @@ struct pyr3_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t samples = 0;
+  // Genomes run through pyr3_iterate, with their own copies of the records.
+  std::vector<pyr3_renderer*> solo_r;
+  std::vector<pyr3_genome> solo_g;
+  std::vector<pyr3_iterate_opts> solo_o;
+  std::vector<std::vector<float>> solo_xf, solo_xaos;
+  std::vector<cudaEvent_t> solo_ev;
 };
 
 namespace {
@@ -813,6 +827,7 @@ void free_batch(pyr3_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   for (auto s : b->streams) cudaStreamDestroy(s);
   for (auto e : b->joins) cudaEventDestroy(e);
+  for (auto e : b->solo_ev) cudaEventDestroy(e);
   if (b->fork) cudaEventDestroy(b->fork);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
@@ -849,8 +864,9 @@ PYR3_API int pyr3_batch_create(pyr3_renderer* const* renderers, const pyr3_genom
   // Modules (one instance per genome of a repeated structure), tables and
   // records, and the launch arguments.
   std::map<std::string, int> seen;
-  std::vector<ChaosArgs> args(n);
-  std::vector<unsigned> grids(n);
+  std::vector<ChaosArgs> args;
+  std::vector<unsigned> grids;
+  std::vector<pyr3_renderer*> graph_r;
   const int sms = device_sms(dev);
   for (uint32_t i = 0; i < n; ++i) {
     pyr3_renderer* r = renderers[i];
@@ -861,9 +877,24 @@ PYR3_API int pyr3_batch_create(pyr3_renderer* const* renderers, const pyr3_genom
     std::string e = pyr3::shape_from_packed(g->xforms, (int)g->n_xforms, g->final_slot, &shape);
     if (!e.empty())
       return fail(e.find("not implemented") != std::string::npos ? PYR3_E_UNSUPPORTED : PYR3_E_INVALID, e);
+    const uint64_t total = o->walkers * o->iters_per_walker;
+    if (!(o->flags & PYR3_ITER_EXACT_WALKERS) && total >= kTuneMinSamples) {
+      const size_t nrec = (size_t)g->n_xforms + (g->final_slot >= 0 ? 1 : 0);
+      b->solo_xf.emplace_back(g->xforms, g->xforms + nrec * 116);
+      b->solo_xaos.emplace_back();
+      if (g->xaos) b->solo_xaos.back().assign(g->xaos, g->xaos + (size_t)g->n_xforms * g->n_xforms);
+      b->solo_r.push_back(r);
+      b->solo_g.push_back(*g);
+      b->solo_o.push_back(*o);
+      cudaEvent_t ev;
+      CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      b->solo_ev.push_back(ev);
+      b->samples += total;
+      continue;
+    }
     const bool aggregate = (o->flags & PYR3_ITER_AGGREGATE) != 0;
     const std::string key = shape.key() + (aggregate ? "|A" : "");
-    const int inst = seen[key]++;
+    const int inst = 1 + seen[key]++;
     std::shared_ptr<pyr3::ChaosModule> m;
     std::string err;
     int rc = pyr3::get_chaos_module(shape, kWpb, aggregate, &m, &err, inst);
@@ -872,7 +903,6 @@ PYR3_API int pyr3_batch_create(pyr3_renderer* const* renderers, const pyr3_genom
     rc = upload_genome(r, g, *m);
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(r->stream));
-    const uint64_t total = o->walkers * o->iters_per_walker;
     ChaosArgs A = base_args(r, g, o);
     uint64_t nw;
     if (o->flags & PYR3_ITER_EXACT_WALKERS) {
@@ -886,17 +916,24 @@ PYR3_API int pyr3_batch_create(pyr3_renderer* const* renderers, const pyr3_genom
     A.n_walkers = nw;
     A.iters_base = total / nw;
     A.iters_extra = total % nw;
-    args[i] = A;
-    grids[i] = (unsigned)std::min<uint64_t>((nw + m->wpb - 1) / m->wpb, (uint64_t)m->blocks_per_sm * sms);
+    args.push_back(A);
+    grids.push_back((unsigned)std::min<uint64_t>((nw + m->wpb - 1) / m->wpb, (uint64_t)m->blocks_per_sm * sms));
+    graph_r.push_back(r);
     b->samples += total;
   }
+  // Pointers into the copies are taken once every copy is in place.
+  for (size_t s = 0; s < b->solo_g.size(); ++s) {
+    b->solo_g[s].xforms = b->solo_xf[s].data();
+    b->solo_g[s].xaos = b->solo_xaos[s].empty() ? nullptr : b->solo_xaos[s].data();
+  }
+  const uint32_t ng = (uint32_t)graph_r.size();
   // Capture: fork to the worker streams, per genome clear + chaos kernel,
   // join back.
   CUDA_TRY(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
   cudaError_t ce = cudaEventRecord(b->fork, b->origin);
   for (uint32_t j = 0; j < k && ce == cudaSuccess; ++j) ce = cudaStreamWaitEvent(b->streams[j], b->fork, 0);
-  for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
-    pyr3_renderer* r = renderers[i];
+  for (uint32_t i = 0; i < ng && ce == cudaSuccess; ++i) {
+    pyr3_renderer* r = graph_r[i];
     cudaStream_t st = b->streams[i % k];
     ce = cudaMemsetAsync(r->d_hist, 0, (size_t)r->SW * r->SH * 16, st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(r->d_counters, 0, 16, st);
@@ -928,6 +965,20 @@ PYR3_API int pyr3_batch_run(pyr3_batch* b) {
   cudaSetDevice(b->device);
   CUDA_TRY(cudaEventRecord(b->ev0, b->origin));
   CUDA_TRY(cudaGraphLaunch(b->exec, b->origin));
+  // Large genomes: one after another (each waits for the previous one's
+  // work), beside the graph.
+  cudaEvent_t prev = b->ev0;
+  for (size_t s = 0; s < b->solo_r.size(); ++s) {
+    pyr3_renderer* r = b->solo_r[s];
+    CUDA_TRY(cudaStreamWaitEvent(r->stream, prev, 0));
+    CUDA_TRY(cudaMemsetAsync(r->d_hist, 0, (size_t)r->SW * r->SH * 16, r->stream));
+    CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, 16, r->stream));
+    const int rc = pyr3_iterate(r, &b->solo_g[s], &b->solo_o[s]);
+    if (rc) return rc;
+    CUDA_TRY(cudaEventRecord(b->solo_ev[s], r->stream));
+    prev = b->solo_ev[s];
+  }
+  if (prev != b->ev0) CUDA_TRY(cudaStreamWaitEvent(b->origin, prev, 0));
   CUDA_TRY(cudaEventRecord(b->ev1, b->origin));
   return PYR3_OK;
 }

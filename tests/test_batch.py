@@ -1,8 +1,9 @@
-"""GPU: batched rendering (pyr3_batch_*): every genome of a batch, rendered
-concurrently by one CUDA graph, agrees with the same genome rendered alone
-through the per-genome path -- statistically, since walker counts and seeds
-differ -- and gets exactly its samples.  Two genomes of the batch share a
-structure, so each needs its own module instance."""
+"""GPU: batched rendering (pyr3_batch_*): every genome of a batch agrees with
+the same genome rendered alone through the per-genome path -- statistically,
+since walker counts and seeds differ -- and gets exactly its samples.  Two
+genomes of the batch share a structure, so each needs its own module
+instance; the last genome is large enough (>= 2^26 samples) to run beside
+the graph through the per-genome path, on a structure the graph also uses."""
 import copy
 
 import numpy as np
@@ -25,13 +26,15 @@ def _genomes():
         x.a, x.b, x.c, x.d, x.e, x.f = (v + float(dv) for v, dv in
                                         zip((x.a, x.b, x.c, x.d, x.e, x.f), rng.uniform(-0.1, 0.1, 6)))
     b, _ = workloads.motion_4k()
-    gs = [a, a2, b]
+    big = copy.deepcopy(a2)
+    gs = [a, a2, b, big]
     for g in gs:
         g.size = (W, H)
         g.oversample = 1
         g.density = None
         g.scale = W / 4
         g.quality = 2560.0  # 4.9e7 samples each
+    big.quality = 3600.0  # 6.9e7 samples: outside the graph
     return gs
 
 
