@@ -36,6 +36,7 @@ CONFIGS = {
     "plain_small": ("iters/s (640x480, 3 xforms)", "plain_small"),
     "motion_4k": ("iters/s (4K, 6 xforms, 8 temporal samples)", "motion_4k"),
     "batch_256": ("iters/s (256 genomes, batched)", "batch_256"),
+    "denoise": ("denoiser training pixels/s (U-Net fwd+bwd+Adam)", "denoise_set"),
 }
 
 
@@ -437,6 +438,93 @@ def bench_reference(args, ws, rank, local, dist):
             "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def bench_denoise(args, ws, rank, local, dist):
+    """Learned denoiser: a step = 50 Adam steps on batches of 8 random
+    128x128 crops from 64 training genomes' (25 spp features, 2000 spp
+    target) renders at 256x256; afterwards the 8 held-out genomes are
+    denoised and scored (PSNR against their 2000-spp renders)."""
+    import time as _t
+
+    import torch
+
+    from pyr3_b200 import denoise as DN
+    from pyr3_b200 import workloads
+
+    gs = workloads.denoise_set(seed=5 + 1000 * rank, n=72, size=256)
+    t0 = _t.perf_counter()
+    xs, ts = DN.make_dataset(gs)
+    render_s = _t.perf_counter() - t0
+    xtr, ttr, xho, tho = xs[:64], ts[:64], xs[64:], ts[64:]
+    per = 50
+    batch, crop = 8, 128
+    net, _, _ = DN.train(xtr, ttr, steps=per * args.warmup, batch=batch, crop=crop, seed=1)
+    params = net.params()
+    torch.cuda.synchronize()
+    _barrier(dist)
+    clocks = Clocks(local) if rank == 0 else None
+    net, losses, ms = DN.train(xtr, ttr, steps=per * args.steps, batch=batch, crop=crop, seed=2,
+                               params=params)
+    launches = net.launches
+    clk = clocks.stop() if clocks else None
+    t_max = _max_over_ranks(ms, dist, local)
+    p_noisy, p_dn, _ = DN.evaluate(net.params(), xho, tho)
+    # e2e: batches assembled on the host, uploaded each step, loss read back each step
+    rng = np.random.default_rng(3)
+    hnet = DN.UNet(batch, crop, crop, net.params())
+    n_e2e = per
+    hx = np.empty((batch, 8, crop, crop), np.float32)
+    ht = np.empty((batch, 3, crop, crop), np.float32)
+    torch.cuda.synchronize()
+    t0 = _t.perf_counter()
+    for _ in range(n_e2e):
+        idx = rng.integers(0, 64, batch)
+        yy, xx = rng.integers(0, 256 - crop + 1, batch), rng.integers(0, 256 - crop + 1, batch)
+        for j in range(batch):
+            hx[j] = xtr[idx[j], :, yy[j]:yy[j] + crop, xx[j]:xx[j] + crop]
+            ht[j] = ttr[idx[j], :, yy[j]:yy[j] + crop, xx[j]:xx[j] + crop]
+        hnet.set_batch(hx, ht)
+        hnet.forward()
+        hnet.loss_and_grad()
+        hnet.backward()
+        hnet.step()
+        hnet.read_loss()
+    e2e_s = _t.perf_counter() - t0
+    e2e_max = _max_over_ranks(e2e_s * 1e3, dist, local)
+    if rank != 0:
+        return None
+    pix_step = batch * crop * crop
+    value = ws * pix_step * per * args.steps / (t_max / 1e3)
+    flop_pix = 3.0 * DN.flops_per_pixel()  # forward + data and weight gradients
+    achieved = value / ws * flop_pix / 1e12
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, pk = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        peak, pk = 1590.0, "fallback"
+    return {
+        "metric": CONFIGS["denoise"][0], "value": value, "unit": "pixels/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (72 seeded genomes, pyr3_b200/workloads.py:denoise_set, rendered here)",
+        "config": {"workload": "denoise", "unet_levels": len(DN.CHANS), "channels": list(DN.CHANS),
+                   "params": DN.param_count(), "canvas": [256, 256], "spp_input": 25, "spp_target": 2000,
+                   "train_genomes": 64, "held_out_genomes": 8, "batch": batch, "crop": crop,
+                   "adam_steps_per_step": per, "l2": "inputs resident; working set < L2 per layer",
+                   "parallelism": f"replicas x{ws}"},
+        "quality": {"held_out_psnr_input_db": p_noisy, "held_out_psnr_denoised_db": p_dn,
+                    "train_loss_first_last": [losses[0][1], losses[-1][1]],
+                    "adam_steps_total": per * (args.warmup + args.steps), "render_seconds": render_s},
+        "e2e": {"value": ws * pix_step * n_e2e / (e2e_max / 1e3), "unit": "pixels/s",
+                "h2d_bytes_per_step": int(hx.nbytes + ht.nbytes) * per, "d2h_bytes_per_step": 4 * per},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "note": f"FLOPs = 3 x 2 x sum(ci co 9 H_l W_l) per pixel = {flop_pix:.0f}; the layers run "
+                             f"in f32 on the CUDA cores (no tensor-core path yet); peak = bf16 dense, {pk}"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -453,9 +541,17 @@ def main():
     args.warmup = max(3, args.warmup)
     ws, rank, local, dist = _dist()
     try:
-        line = bench_reference(args, ws, rank, local, dist) if args.impl == "reference" else \
-            bench_batch(args, ws, rank, local, dist) if args.config == "batch_256" else \
-            bench_ours(args, ws, rank, local, dist)
+        if args.impl == "reference" and args.config == "denoise":
+            line = {"impl": "reference", "unavailable": "the reference has no learned denoiser"} \
+                if rank == 0 else None
+        elif args.impl == "reference":
+            line = bench_reference(args, ws, rank, local, dist)
+        elif args.config == "batch_256":
+            line = bench_batch(args, ws, rank, local, dist)
+        elif args.config == "denoise":
+            line = bench_denoise(args, ws, rank, local, dist)
+        else:
+            line = bench_ours(args, ws, rank, local, dist)
         if line is not None:
             print(json.dumps(line))
     finally:

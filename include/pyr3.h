@@ -251,6 +251,51 @@ int pyr3_density_tonemap_noalloc(const uint32_t *device_hist, uint32_t width, ui
  * returns the NVRTC log on failure via pyr3_last_error. */
 int pyr3_prepare(pyr3_renderer *r, const pyr3_genome *g);
 
+/* ---- learned denoiser layers ---------------------------------------- */
+/* No counterpart in the reference: the denoiser is an addition.  Layers of
+ * a U-Net over device tensors, NCHW f32; each operand is a device pointer
+ * plus its per-image stride in floats, so a channel slice of a larger
+ * tensor (a skip concatenation) is a valid operand.  Work is queued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream).  Errors:
+ * PYR3_E_INVALID for null operands or bad sizes, PYR3_E_CUDA for launch
+ * failures. */
+/* out[n,co] = bias[co] + sum_ci conv3x3(in[n,ci], weight[co][ci]), zero
+ * padding; ReLU if relu.  weight is [co][ci][3][3]; bias may be NULL. */
+int pyr3_dn_conv3x3(const float *in, int64_t in_ns, int32_t ci, float *out, int64_t out_ns,
+                    int32_t co, int32_t n, int32_t h, int32_t w, const float *weight,
+                    const float *bias, int32_t relu, void *stream);
+/* Weight (and, if dbias is not NULL, bias) gradient of pyr3_dn_conv3x3
+ * given its input and the gradient of its output; overwrites. */
+int pyr3_dn_conv3x3_wgrad(const float *in, int64_t in_ns, int32_t ci, const float *dout,
+                          int64_t dout_ns, int32_t co, int32_t n, int32_t h, int32_t w,
+                          float *dweight, float *dbias, void *stream);
+/* flipped[ci][co][k] = weight[co][ci][8-k]: pyr3_dn_conv3x3 with these
+ * weights (co and ci swapped, no bias) maps an output gradient to the
+ * input gradient. */
+int pyr3_dn_flip_weights(const float *weight, int32_t co, int32_t ci, float *flipped, void *stream);
+/* grad = 0 wherever y <= 0 (ReLU backward), c channels of hw pixels. */
+int pyr3_dn_relu_mask(float *grad, int64_t grad_ns, const float *y, int64_t y_ns, int32_t c,
+                      int32_t n, int32_t hw, void *stream);
+/* y += x over c channels of hw pixels. */
+int pyr3_dn_add(float *y, int64_t y_ns, const float *x, int64_t x_ns, int32_t c, int32_t n,
+                int32_t hw, void *stream);
+/* 2x2 average pool of an h x w input (h, w even); with backward, in is the
+ * (h/2 x w/2) output gradient and out the h x w input gradient, written or,
+ * with accumulate, added. */
+int pyr3_dn_pool2(const float *in, int64_t in_ns, float *out, int64_t out_ns, int32_t c, int32_t n,
+                  int32_t h, int32_t w, int32_t backward, int32_t accumulate, void *stream);
+/* Nearest 2x upsample of an h x w input; with backward, in is the
+ * (2h x 2w) output gradient and out the h x w input gradient. */
+int pyr3_dn_up2(const float *in, int64_t in_ns, float *out, int64_t out_ns, int32_t c, int32_t n,
+                int32_t h, int32_t w, int32_t backward, void *stream);
+/* grad = 2 (pred - target) / count; *loss_sum += sum (pred - target)^2
+ * (device float, zeroed by the caller). */
+int pyr3_dn_mse(const float *pred, const float *target, int64_t count, float *grad,
+                float *loss_sum, void *stream);
+/* One bias-corrected Adam step (step >= 1) over count parameters. */
+int pyr3_dn_adam(float *param, const float *grad, float *m, float *v, int64_t count, float lr,
+                 float beta1, float beta2, float eps, int32_t step, void *stream);
+
 /* ---- build checks (no GPU needed) ------------------------------------ */
 /* Generate + NVRTC-compile the chaos kernel for a genome structure without
  * touching a device; *cubin_bytes receives the image size. */

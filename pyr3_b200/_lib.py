@@ -87,6 +87,23 @@ _SIGS = {
     "pyr3_counters": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "pyr3_last_iterate_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "pyr3_last_iterate_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "pyr3_dn_conv3x3": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_int64, C.c_int32,
+                                  C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                  C.c_void_p]),
+    "pyr3_dn_conv3x3_wgrad": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_int64, C.c_int32,
+                                        C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pyr3_dn_flip_weights": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    "pyr3_dn_relu_mask": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
+                                    C.c_int32, C.c_void_p]),
+    "pyr3_dn_add": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                              C.c_void_p]),
+    "pyr3_dn_pool2": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                                C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
+    "pyr3_dn_up2": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                              C.c_int32, C.c_int32, C.c_void_p]),
+    "pyr3_dn_mse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pyr3_dn_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float,
+                               C.c_float, C.c_float, C.c_int32, C.c_void_p]),
     "pyr3_mark": (C.c_int, [C.c_void_p, C.c_int32]),
     "pyr3_elapsed": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_float)]),
     "pyr3_flush_l2": (C.c_int, [C.c_void_p, C.c_uint64]),

@@ -5,8 +5,9 @@
    implements, found by scanning the VAR(...) / DCV(...) definitions) into
    csrc/gen/jit_sources.inc.
 2. nvcc -gencode arch=compute_100a,code=sm_100a the C-ABI (capi.cpp), the
-   JIT driver (jit.cpp), the density / tonemap passes (passes.cu) and the
-   fixed scratch of the allocation-free present (noalloc.cu).
+   JIT driver (jit.cpp), the density / tonemap passes (passes.cu), the
+   fixed scratch of the allocation-free present (noalloc.cu) and the
+   denoiser layers (denoise.cu).
 """
 from __future__ import annotations
 
@@ -82,9 +83,10 @@ def generate_sources() -> str:
 
 def build(force: bool = False) -> str:
     inc = generate_sources()
-    srcs = [os.path.join(CSRC, f) for f in ("capi.cpp", "jit.cpp", "passes.cu", "noalloc.cu")]
+    srcs = [os.path.join(CSRC, f) for f in ("capi.cpp", "jit.cpp", "passes.cu", "noalloc.cu", "denoise.cu")]
     deps = srcs + [inc, os.path.join(ROOT, "include", "pyr3.h"), os.path.join(CSRC, "jit.h"),
-                   os.path.join(CSRC, "passes.h"), os.path.join(CSRC, "noalloc.h")]
+                   os.path.join(CSRC, "passes.h"), os.path.join(CSRC, "noalloc.h"),
+                   os.path.join(CSRC, "denoise.h")]
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
         return LIB
     cmd = [NVCC, "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "jit.h"
+#include "denoise.h"
 #include "noalloc.h"
 #include "passes.h"
 #include "pyr3.h"
@@ -997,6 +998,92 @@ PYR3_API int pyr3_batch_destroy(pyr3_batch* b) {
   cudaSetDevice(b->device);
   cudaStreamSynchronize(b->origin);
   free_batch(b);
+  return PYR3_OK;
+}
+
+// ---------------------------------------------------------------- denoiser
+// Layers of the learned denoiser's U-Net on device tensors (NCHW f32, each
+// operand a pointer plus per-image stride).  Argument checks only; the
+// shapes' consistency with the buffers is the caller's.
+namespace {
+bool dn_dims_ok(int64_t a, int64_t b, int64_t c, int64_t d) { return a > 0 && b > 0 && c > 0 && d > 0; }
+}  // namespace
+
+PYR3_API int pyr3_dn_conv3x3(const float* in, int64_t in_ns, int32_t ci, float* out, int64_t out_ns,
+                             int32_t co, int32_t n, int32_t h, int32_t w, const float* weight,
+                             const float* bias, int32_t relu, void* stream) {
+  if (!in || !out || !weight || !dn_dims_ok(ci, co, n, (int64_t)h * w) || h <= 0 || w <= 0)
+    return fail(PYR3_E_INVALID, "conv3x3: null operand or non-positive size");
+  CUDA_TRY(pyr3::dn_conv3x3(in, in_ns, ci, out, out_ns, co, n, h, w, weight, bias, relu != 0,
+                            (cudaStream_t)stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_dn_conv3x3_wgrad(const float* in, int64_t in_ns, int32_t ci, const float* dout,
+                                   int64_t dout_ns, int32_t co, int32_t n, int32_t h, int32_t w,
+                                   float* dweight, float* dbias, void* stream) {
+  if (!in || !dout || !dweight || !dn_dims_ok(ci, co, n, (int64_t)h * w) || h <= 0 || w <= 0)
+    return fail(PYR3_E_INVALID, "conv3x3_wgrad: null operand or non-positive size");
+  CUDA_TRY(pyr3::dn_conv3x3_wgrad(in, in_ns, ci, dout, dout_ns, co, n, h, w, dweight, dbias,
+                                  (cudaStream_t)stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_dn_flip_weights(const float* weight, int32_t co, int32_t ci, float* flipped,
+                                  void* stream) {
+  if (!weight || !flipped || co <= 0 || ci <= 0)
+    return fail(PYR3_E_INVALID, "flip_weights: null operand or non-positive size");
+  CUDA_TRY(pyr3::dn_flip_weights(weight, co, ci, flipped, (cudaStream_t)stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_dn_relu_mask(float* grad, int64_t grad_ns, const float* y, int64_t y_ns, int32_t c,
+                               int32_t n, int32_t hw, void* stream) {
+  if (!grad || !y || !dn_dims_ok(c, n, hw, 1)) return fail(PYR3_E_INVALID, "relu_mask: bad arguments");
+  CUDA_TRY(pyr3::dn_relu_mask(grad, grad_ns, y, y_ns, c, n, hw, (cudaStream_t)stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_dn_add(float* y, int64_t y_ns, const float* x, int64_t x_ns, int32_t c, int32_t n,
+                         int32_t hw, void* stream) {
+  if (!y || !x || !dn_dims_ok(c, n, hw, 1)) return fail(PYR3_E_INVALID, "add: bad arguments");
+  CUDA_TRY(pyr3::dn_add(y, y_ns, x, x_ns, c, n, hw, (cudaStream_t)stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_dn_pool2(const float* in, int64_t in_ns, float* out, int64_t out_ns, int32_t c,
+                           int32_t n, int32_t h, int32_t w, int32_t backward, int32_t accumulate,
+                           void* stream) {
+  if (!in || !out || !dn_dims_ok(c, n, h, w) || (h & 1) || (w & 1))
+    return fail(PYR3_E_INVALID, "pool2: null operand, non-positive size or odd height/width");
+  if (backward)
+    CUDA_TRY(pyr3::dn_pool2_bwd(in, in_ns, out, out_ns, c, n, h, w, accumulate != 0, (cudaStream_t)stream));
+  else
+    CUDA_TRY(pyr3::dn_pool2(in, in_ns, out, out_ns, c, n, h, w, (cudaStream_t)stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_dn_up2(const float* in, int64_t in_ns, float* out, int64_t out_ns, int32_t c,
+                         int32_t n, int32_t h, int32_t w, int32_t backward, void* stream) {
+  if (!in || !out || !dn_dims_ok(c, n, h, w)) return fail(PYR3_E_INVALID, "up2: bad arguments");
+  if (backward)
+    CUDA_TRY(pyr3::dn_up2_bwd(in, in_ns, out, out_ns, c, n, h, w, (cudaStream_t)stream));
+  else
+    CUDA_TRY(pyr3::dn_up2(in, in_ns, out, out_ns, c, n, h, w, (cudaStream_t)stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_dn_mse(const float* pred, const float* target, int64_t count, float* grad,
+                         float* loss_sum, void* stream) {
+  if (!pred || !target || !grad || !loss_sum || count <= 0) return fail(PYR3_E_INVALID, "mse: bad arguments");
+  CUDA_TRY(pyr3::dn_mse(pred, target, count, grad, loss_sum, (cudaStream_t)stream));
+  return PYR3_OK;
+}
+
+PYR3_API int pyr3_dn_adam(float* param, const float* grad, float* m, float* v, int64_t count, float lr,
+                          float beta1, float beta2, float eps, int32_t step, void* stream) {
+  if (!param || !grad || !m || !v || count <= 0 || step < 1) return fail(PYR3_E_INVALID, "adam: bad arguments");
+  CUDA_TRY(pyr3::dn_adam(param, grad, m, v, count, lr, beta1, beta2, eps, step, (cudaStream_t)stream));
   return PYR3_OK;
 }
 

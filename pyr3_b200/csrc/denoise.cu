@@ -1,0 +1,315 @@
+// Denoiser kernels (see denoise.h).  f32 on the CUDA cores: the
+// convolution stages a 16 x 16 output tile (+1 halo) of 4 input channels and
+// the matching 8 x 4 x 9 weights in shared memory per step; each thread
+// accumulates 8 output channels of one pixel.
+#include "denoise.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace pyr3 {
+namespace {
+
+constexpr int TS = 16;    // output tile edge
+constexpr int CO_B = 8;   // output channels per block
+constexpr int CI_B = 4;   // input channels staged per step
+
+__global__ void __launch_bounds__(256)
+k_conv3x3(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __restrict__ out,
+          int64_t out_ns, int co_n, int H, int W, const float* __restrict__ wt,
+          const float* __restrict__ bias, int relu) {
+  __shared__ float tile[CI_B][TS + 2][TS + 3];
+  __shared__ float ws[CI_B][9][CO_B];
+  const int tx = threadIdx.x & (TS - 1), ty = threadIdx.x / TS;
+  const int x0 = blockIdx.x * TS, y0 = blockIdx.y * TS;
+  const int groups = (co_n + CO_B - 1) / CO_B;
+  const int n = blockIdx.z / groups, co0 = (blockIdx.z % groups) * CO_B;
+  const int64_t hw = (int64_t)H * W;
+  const float* inn = in + n * in_ns;
+  float acc[CO_B];
+#pragma unroll
+  for (int j = 0; j < CO_B; ++j) acc[j] = 0.0f;
+  for (int c0 = 0; c0 < ci_n; c0 += CI_B) {
+    for (int i = threadIdx.x; i < CI_B * (TS + 2) * (TS + 2); i += 256) {
+      const int c = i / ((TS + 2) * (TS + 2)), r = i % ((TS + 2) * (TS + 2));
+      const int yy = r / (TS + 2), xx = r % (TS + 2);
+      const int gy = y0 + yy - 1, gx = x0 + xx - 1;
+      float v = 0.0f;
+      if (c0 + c < ci_n && gy >= 0 && gy < H && gx >= 0 && gx < W)
+        v = inn[(c0 + c) * hw + (int64_t)gy * W + gx];
+      tile[c][yy][xx] = v;
+    }
+    for (int i = threadIdx.x; i < CO_B * CI_B * 9; i += 256) {
+      const int j = i / (CI_B * 9), r = i % (CI_B * 9), c = r / 9, k = r % 9;
+      float v = 0.0f;
+      if (co0 + j < co_n && c0 + c < ci_n) v = wt[((int64_t)(co0 + j) * ci_n + c0 + c) * 9 + k];
+      ws[c][k][j] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < CI_B; ++c) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const float v = tile[c][ty + k / 3][tx + k % 3];
+#pragma unroll
+        for (int j = 0; j < CO_B; ++j) acc[j] = fmaf(ws[c][k][j], v, acc[j]);
+      }
+    }
+    __syncthreads();
+  }
+  const int x = x0 + tx, y = y0 + ty;
+  if (x >= W || y >= H) return;
+#pragma unroll
+  for (int j = 0; j < CO_B; ++j) {
+    if (co0 + j >= co_n) break;
+    float r = acc[j] + (bias ? bias[co0 + j] : 0.0f);
+    if (relu) r = fmaxf(r, 0.0f);
+    out[n * out_ns + (co0 + j) * hw + (int64_t)y * W + x] = r;
+  }
+}
+
+// Block (ci, co) reduces the 9 taps over every pixel of every image.
+__global__ void __launch_bounds__(256)
+k_conv3x3_wgrad(const float* __restrict__ in, int64_t in_ns, int ci_n,
+                const float* __restrict__ dout, int64_t dout_ns, int n_img, int H, int W,
+                float* __restrict__ dw) {
+  const int ci = blockIdx.x, co = blockIdx.y;
+  const int64_t hw = (int64_t)H * W;
+  float a[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) a[k] = 0.0f;
+  for (int n = 0; n < n_img; ++n) {
+    const float* g = dout + n * dout_ns + co * hw;
+    const float* ip = in + n * in_ns + ci * hw;
+    for (int64_t p = threadIdx.x; p < hw; p += blockDim.x) {
+      const float gv = g[p];
+      if (gv == 0.0f) continue;  // ReLU-masked gradients are often zero
+      const int y = (int)(p / W), x = (int)(p % W);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const int gy = y + k / 3 - 1, gx = x + k % 3 - 1;
+        if (gy >= 0 && gy < H && gx >= 0 && gx < W) a[k] = fmaf(gv, ip[(int64_t)gy * W + gx], a[k]);
+      }
+    }
+  }
+  __shared__ float red[9][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    float v = a[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 9) {
+    float v = 0.0f;
+    for (int j = 0; j < (int)(blockDim.x >> 5); ++j) v += red[threadIdx.x][j];
+    dw[((int64_t)co * ci_n + ci) * 9 + threadIdx.x] = v;
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_bias_grad(const float* __restrict__ dout, int64_t dout_ns, int n_img, int64_t hw, float* db) {
+  const int co = blockIdx.x;
+  float a = 0.0f;
+  for (int n = 0; n < n_img; ++n)
+    for (int64_t p = threadIdx.x; p < hw; p += blockDim.x) a += dout[n * dout_ns + co * hw + p];
+  __shared__ float red[8];
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float v = 0.0f;
+    for (int j = 0; j < (int)(blockDim.x >> 5); ++j) v += red[j];
+    db[co] = v;
+  }
+}
+
+__global__ void k_flip(const float* __restrict__ w, int co_n, int ci_n, float* __restrict__ wt) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)co_n * ci_n * 9) return;
+  const int k = (int)(i % 9);
+  const int64_t r = i / 9;
+  const int ci = (int)(r % ci_n), co = (int)(r / ci_n);
+  wt[((int64_t)ci * co_n + co) * 9 + (8 - k)] = w[i];
+}
+
+// Element i of c channels x hw pixels of image n lives at n * ns + i.
+__global__ void k_relu_mask(float* g, int64_t g_ns, const float* __restrict__ y, int64_t y_ns,
+                            int64_t per, int n_img) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= per * n_img) return;
+  const int64_t n = i / per, r = i % per;
+  if (!(y[n * y_ns + r] > 0.0f)) g[n * g_ns + r] = 0.0f;
+}
+
+__global__ void k_add(float* y, int64_t y_ns, const float* __restrict__ x, int64_t x_ns, int64_t per,
+                      int n_img) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= per * n_img) return;
+  const int64_t n = i / per, r = i % per;
+  y[n * y_ns + r] += x[n * x_ns + r];
+}
+
+// One thread per output pixel of the half-size plane.
+__global__ void k_pool2(const float* __restrict__ in, int64_t in_ns, float* out, int64_t out_ns, int c_n,
+                        int n_img, int H, int W) {
+  const int h2 = H / 2, w2 = W / 2;
+  const int64_t per = (int64_t)c_n * h2 * w2;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= per * n_img) return;
+  const int64_t n = i / per, r = i % per;
+  const int64_t c = r / ((int64_t)h2 * w2), q = r % ((int64_t)h2 * w2);
+  const int y = (int)(q / w2), x = (int)(q % w2);
+  const float* p = in + n * in_ns + c * H * W + (int64_t)(2 * y) * W + 2 * x;
+  out[n * out_ns + r] = 0.25f * ((p[0] + p[1]) + (p[W] + p[W + 1]));
+}
+
+__global__ void k_pool2_bwd(const float* __restrict__ dout, int64_t dout_ns, float* din, int64_t din_ns,
+                            int c_n, int n_img, int H, int W, int accumulate) {
+  const int h2 = H / 2, w2 = W / 2;
+  const int64_t per = (int64_t)c_n * h2 * w2;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= per * n_img) return;
+  const int64_t n = i / per, r = i % per;
+  const int64_t c = r / ((int64_t)h2 * w2), q = r % ((int64_t)h2 * w2);
+  const int y = (int)(q / w2), x = (int)(q % w2);
+  const float g = 0.25f * dout[n * dout_ns + r];
+  float* p = din + n * din_ns + c * H * W + (int64_t)(2 * y) * W + 2 * x;
+  if (accumulate) {
+    p[0] += g; p[1] += g; p[W] += g; p[W + 1] += g;
+  } else {
+    p[0] = g; p[1] = g; p[W] = g; p[W + 1] = g;
+  }
+}
+
+// in is h x w; one thread per input pixel writes its 2 x 2 block.
+__global__ void k_up2(const float* __restrict__ in, int64_t in_ns, float* out, int64_t out_ns, int c_n,
+                      int n_img, int H, int W) {
+  const int64_t per = (int64_t)c_n * H * W;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= per * n_img) return;
+  const int64_t n = i / per, r = i % per;
+  const int64_t c = r / ((int64_t)H * W), q = r % ((int64_t)H * W);
+  const int y = (int)(q / W), x = (int)(q % W);
+  const float v = in[n * in_ns + r];
+  float* p = out + n * out_ns + c * 4 * H * W + (int64_t)(2 * y) * (2 * W) + 2 * x;
+  p[0] = v; p[1] = v; p[2 * W] = v; p[2 * W + 1] = v;
+}
+
+__global__ void k_up2_bwd(const float* __restrict__ dout, int64_t dout_ns, float* din, int64_t din_ns,
+                          int c_n, int n_img, int H, int W) {
+  const int64_t per = (int64_t)c_n * H * W;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= per * n_img) return;
+  const int64_t n = i / per, r = i % per;
+  const int64_t c = r / ((int64_t)H * W), q = r % ((int64_t)H * W);
+  const int y = (int)(q / W), x = (int)(q % W);
+  const float* p = dout + n * dout_ns + c * 4 * H * W + (int64_t)(2 * y) * (2 * W) + 2 * x;
+  din[n * din_ns + r] = (p[0] + p[1]) + (p[2 * W] + p[2 * W + 1]);
+}
+
+__global__ void __launch_bounds__(256)
+k_mse(const float* __restrict__ pred, const float* __restrict__ tgt, int64_t count, float* grad,
+      float* loss_sum) {
+  float a = 0.0f;
+  const float sc = 2.0f / (float)count;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float d = pred[i] - tgt[i];
+    grad[i] = sc * d;
+    a = fmaf(d, d, a);
+  }
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss_sum, a);
+}
+
+__global__ void k_adam(float* p, const float* __restrict__ g, float* m, float* v, int64_t count,
+                       float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+unsigned blocks_for(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace
+
+cudaError_t dn_conv3x3(const float* in, int64_t in_ns, int ci, float* out, int64_t out_ns, int co, int n,
+                       int h, int w, const float* weight, const float* bias, bool relu, cudaStream_t s) {
+  const dim3 grid((w + TS - 1) / TS, (h + TS - 1) / TS, n * ((co + CO_B - 1) / CO_B));
+  k_conv3x3<<<grid, 256, 0, s>>>(in, in_ns, ci, out, out_ns, co, h, w, weight, bias, relu ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_conv3x3_wgrad(const float* in, int64_t in_ns, int ci, const float* dout, int64_t dout_ns,
+                             int co, int n, int h, int w, float* dw, float* db, cudaStream_t s) {
+  k_conv3x3_wgrad<<<dim3(ci, co), 256, 0, s>>>(in, in_ns, ci, dout, dout_ns, n, h, w, dw);
+  if (db) k_bias_grad<<<co, 256, 0, s>>>(dout, dout_ns, n, (int64_t)h * w, db);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_flip_weights(const float* w, int co, int ci, float* wt, cudaStream_t s) {
+  k_flip<<<blocks_for((int64_t)co * ci * 9), 256, 0, s>>>(w, co, ci, wt);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_relu_mask(float* g, int64_t g_ns, const float* y, int64_t y_ns, int c, int n, int hw,
+                         cudaStream_t s) {
+  const int64_t per = (int64_t)c * hw;
+  k_relu_mask<<<blocks_for(per * n), 256, 0, s>>>(g, g_ns, y, y_ns, per, n);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_add(float* y, int64_t y_ns, const float* x, int64_t x_ns, int c, int n, int hw,
+                   cudaStream_t s) {
+  const int64_t per = (int64_t)c * hw;
+  k_add<<<blocks_for(per * n), 256, 0, s>>>(y, y_ns, x, x_ns, per, n);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_pool2(const float* in, int64_t in_ns, float* out, int64_t out_ns, int c, int n, int h, int w,
+                     cudaStream_t s) {
+  k_pool2<<<blocks_for((int64_t)c * (h / 2) * (w / 2) * n), 256, 0, s>>>(in, in_ns, out, out_ns, c, n, h, w);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_pool2_bwd(const float* dout, int64_t dout_ns, float* din, int64_t din_ns, int c, int n, int h,
+                         int w, bool accumulate, cudaStream_t s) {
+  k_pool2_bwd<<<blocks_for((int64_t)c * (h / 2) * (w / 2) * n), 256, 0, s>>>(dout, dout_ns, din, din_ns, c, n,
+                                                                            h, w, accumulate ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_up2(const float* in, int64_t in_ns, float* out, int64_t out_ns, int c, int n, int h, int w,
+                   cudaStream_t s) {
+  k_up2<<<blocks_for((int64_t)c * h * w * n), 256, 0, s>>>(in, in_ns, out, out_ns, c, n, h, w);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_up2_bwd(const float* dout, int64_t dout_ns, float* din, int64_t din_ns, int c, int n, int h,
+                       int w, cudaStream_t s) {
+  k_up2_bwd<<<blocks_for((int64_t)c * h * w * n), 256, 0, s>>>(dout, dout_ns, din, din_ns, c, n, h, w);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_mse(const float* pred, const float* target, int64_t count, float* grad, float* loss_sum,
+                   cudaStream_t s) {
+  const unsigned b = (unsigned)std::min<int64_t>(blocks_for(count), 148 * 8);
+  k_mse<<<b, 256, 0, s>>>(pred, target, count, grad, loss_sum);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_adam(float* p, const float* g, float* m, float* v, int64_t count, float lr, float b1, float b2,
+                    float eps, int step, cudaStream_t s) {
+  const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+  k_adam<<<blocks_for(count), 256, 0, s>>>(p, g, m, v, count, lr, b1, b2, eps, c1, c2);
+  return cudaGetLastError();
+}
+
+}  // namespace pyr3

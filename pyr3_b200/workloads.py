@@ -162,6 +162,38 @@ def batch_256(seed: int = 4, n: int = 256):
     return out
 
 
+def denoise_set(seed: int = 5, n: int = 72, size: int = 256, structures: int = 4):
+    """Genomes for the learned denoiser: `structures` xform/variation layouts
+    (4, 6, 8 and 12 xforms of 1-2 flam3-core variations each), and for every
+    genome fresh affines, weights, variation weights and parameters, colours
+    and palette on one of them.  Few structures keep the number of compiled
+    chaos modules small; size x size canvases, oversample 1."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    shapes = []
+    for k in range(structures):
+        nx = (4, 6, 8, 12)[k % 4]
+        shapes.append([[int(FLAM3_CORE[int(rng.integers(0, len(FLAM3_CORE)))])
+                        for _ in range(int(rng.integers(1, 3)))] for _ in range(nx)])
+    out = []
+    for i in range(n):
+        sh = shapes[i % structures]
+        weights = rng.dirichlet(np.ones(len(sh)))
+        xforms = []
+        for vars_, w in zip(sh, weights):
+            vw = rng.uniform(0.2, 1.0, len(vars_))
+            vw = vw / vw.sum()
+            vs = [Variation(idx, float(vw[k]), _params_for(rng, idx)) for k, idx in enumerate(vars_)]
+            a, b, c, d, e, f = _random_affine(rng)
+            xforms.append(Xform(a=a, b=b, c=c, d=d, e=e, f=f, weight=float(w),
+                                color=float(rng.uniform(0, 1)), color_speed=float(rng.uniform(0.2, 0.8)),
+                                variations=vs))
+        out.append(Genome(name=f"denoise-{i}", xforms=xforms, scale=size / 4, palette=_hsv_palette(rng),
+                          quality=25, oversample=1, size=(size, size),
+                          tonemap={"gamma": 4.0, "vibrancy": 1.0, "highlightPower": 1.0,
+                                   "brightness": 4.0, "gammaThreshold": 0.01}))
+    return out
+
+
 def write_all(outdir: str | None = None) -> None:
     outdir = outdir or os.path.join(HERE, "workloads")
     os.makedirs(outdir, exist_ok=True)
