@@ -471,6 +471,7 @@ def bench_denoise(args, ws, rank, local, dist):
     # e2e: batches assembled on the host, uploaded each step, loss read back each step
     rng = np.random.default_rng(3)
     hnet = DN.UNet(batch, crop, crop, net.params())
+    hnet.capture()
     n_e2e = per
     hx = np.empty((batch, 8, crop, crop), np.float32)
     ht = np.empty((batch, 3, crop, crop), np.float32)
@@ -483,9 +484,7 @@ def bench_denoise(args, ws, rank, local, dist):
             hx[j] = xtr[idx[j], :, yy[j]:yy[j] + crop, xx[j]:xx[j] + crop]
             ht[j] = ttr[idx[j], :, yy[j]:yy[j] + crop, xx[j]:xx[j] + crop]
         hnet.set_batch(hx, ht)
-        hnet.forward()
-        hnet.loss_and_grad()
-        hnet.backward()
+        hnet.replay()
         hnet.step()
         hnet.read_loss()
     e2e_s = _t.perf_counter() - t0

@@ -265,10 +265,17 @@ int pyr3_dn_conv3x3(const float *in, int64_t in_ns, int32_t ci, float *out, int6
                     int32_t co, int32_t n, int32_t h, int32_t w, const float *weight,
                     const float *bias, int32_t relu, void *stream);
 /* Weight (and, if dbias is not NULL, bias) gradient of pyr3_dn_conv3x3
- * given its input and the gradient of its output; overwrites. */
+ * given its input and the gradient of its output; overwrites.  The sum
+ * over pixels is split into partials held in `scratch`, a device buffer
+ * of at least pyr3_dn_wgrad_scratch_floats(co, ci) floats (PYR3_E_INVALID
+ * if smaller), and added in a fixed order, so the result is reproducible. */
 int pyr3_dn_conv3x3_wgrad(const float *in, int64_t in_ns, int32_t ci, const float *dout,
                           int64_t dout_ns, int32_t co, int32_t n, int32_t h, int32_t w,
-                          float *dweight, float *dbias, void *stream);
+                          float *dweight, float *dbias, float *scratch, uint64_t scratch_floats,
+                          void *stream);
+/* Floats of scratch pyr3_dn_conv3x3_wgrad needs for co x ci channels (0 for
+ * non-positive sizes). */
+uint64_t pyr3_dn_wgrad_scratch_floats(int32_t co, int32_t ci);
 /* flipped[ci][co][k] = weight[co][ci][8-k]: pyr3_dn_conv3x3 with these
  * weights (co and ci swapped, no bias) maps an output gradient to the
  * input gradient. */

@@ -1021,12 +1021,19 @@ PYR3_API int pyr3_dn_conv3x3(const float* in, int64_t in_ns, int32_t ci, float* 
 
 PYR3_API int pyr3_dn_conv3x3_wgrad(const float* in, int64_t in_ns, int32_t ci, const float* dout,
                                    int64_t dout_ns, int32_t co, int32_t n, int32_t h, int32_t w,
-                                   float* dweight, float* dbias, void* stream) {
-  if (!in || !dout || !dweight || !dn_dims_ok(ci, co, n, (int64_t)h * w) || h <= 0 || w <= 0)
+                                   float* dweight, float* dbias, float* scratch, uint64_t scratch_floats,
+                                   void* stream) {
+  if (!in || !dout || !dweight || !scratch || !dn_dims_ok(ci, co, n, (int64_t)h * w) || h <= 0 || w <= 0)
     return fail(PYR3_E_INVALID, "conv3x3_wgrad: null operand or non-positive size");
-  CUDA_TRY(pyr3::dn_conv3x3_wgrad(in, in_ns, ci, dout, dout_ns, co, n, h, w, dweight, dbias,
+  if (scratch_floats < pyr3::dn_wgrad_scratch_floats(co, ci))
+    return fail(PYR3_E_INVALID, "conv3x3_wgrad: scratch smaller than pyr3_dn_wgrad_scratch_floats");
+  CUDA_TRY(pyr3::dn_conv3x3_wgrad(in, in_ns, ci, dout, dout_ns, co, n, h, w, dweight, dbias, scratch,
                                   (cudaStream_t)stream));
   return PYR3_OK;
+}
+
+PYR3_API uint64_t pyr3_dn_wgrad_scratch_floats(int32_t co, int32_t ci) {
+  return co > 0 && ci > 0 ? (uint64_t)pyr3::dn_wgrad_scratch_floats(co, ci) : 0;
 }
 
 PYR3_API int pyr3_dn_flip_weights(const float* weight, int32_t co, int32_t ci, float* flipped,

@@ -13,6 +13,7 @@ namespace {
 constexpr int TS = 16;    // output tile edge
 constexpr int CO_B = 8;   // output channels per block
 constexpr int CI_B = 4;   // input channels staged per step
+constexpr int kWgChunks = 32;  // pixel chunks of the weight gradient
 
 __global__ void __launch_bounds__(256)
 k_conv3x3(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __restrict__ out,
@@ -68,61 +69,81 @@ k_conv3x3(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __restri
   }
 }
 
-// Block (ci, co) reduces the 9 taps over every pixel of every image.
+// Weight and bias gradient, split over pixels: block (ci group of 4, co
+// group of 2, chunk s) accumulates the 2 x 4 x 9 taps (and, for the first
+// ci group, the 2 bias sums) over pixel chunk s of all images into
+// part[s]; k_wgrad_reduce adds the kWgChunks partials in a fixed order.
+constexpr int WG_CI = 4, WG_CO = 2;
+
 __global__ void __launch_bounds__(256)
-k_conv3x3_wgrad(const float* __restrict__ in, int64_t in_ns, int ci_n,
-                const float* __restrict__ dout, int64_t dout_ns, int n_img, int H, int W,
-                float* __restrict__ dw) {
-  const int ci = blockIdx.x, co = blockIdx.y;
-  const int64_t hw = (int64_t)H * W;
-  float a[9];
+k_wgrad_part(const float* __restrict__ in, int64_t in_ns, int ci_n, const float* __restrict__ dout,
+             int64_t dout_ns, int co_n, int n_img, int H, int W, float* __restrict__ part,
+             float* __restrict__ part_b) {
+  const int ci0 = blockIdx.x * WG_CI, co0 = blockIdx.y * WG_CO, s = blockIdx.z;
+  const int64_t hw = (int64_t)H * W, P = hw * n_img;
+  const int64_t p0 = P * s / kWgChunks, p1 = P * (s + 1) / kWgChunks;
+  float a[WG_CO][WG_CI][9], b[WG_CO];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) a[k] = 0.0f;
-  for (int n = 0; n < n_img; ++n) {
-    const float* g = dout + n * dout_ns + co * hw;
-    const float* ip = in + n * in_ns + ci * hw;
-    for (int64_t p = threadIdx.x; p < hw; p += blockDim.x) {
-      const float gv = g[p];
-      if (gv == 0.0f) continue;  // ReLU-masked gradients are often zero
-      const int y = (int)(p / W), x = (int)(p % W);
+  for (int j = 0; j < WG_CO; ++j) {
+    b[j] = 0.0f;
+#pragma unroll
+    for (int c = 0; c < WG_CI; ++c)
+#pragma unroll
+      for (int k = 0; k < 9; ++k) a[j][c][k] = 0.0f;
+  }
+  for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+    const int64_t n = p / hw, r = p % hw;
+    const int y = (int)(r / W), x = (int)(r % W);
+    float g[WG_CO];
+#pragma unroll
+    for (int j = 0; j < WG_CO; ++j) g[j] = co0 + j < co_n ? dout[n * dout_ns + (co0 + j) * hw + r] : 0.0f;
+    if (g[0] == 0.0f && g[1] == 0.0f) continue;  // ReLU-masked gradients are often zero
+#pragma unroll
+    for (int j = 0; j < WG_CO; ++j) b[j] += g[j];
+#pragma unroll
+    for (int c = 0; c < WG_CI; ++c) {
+      if (ci0 + c >= ci_n) break;
+      const float* ip = in + n * in_ns + (ci0 + c) * hw;
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
         const int gy = y + k / 3 - 1, gx = x + k % 3 - 1;
-        if (gy >= 0 && gy < H && gx >= 0 && gx < W) a[k] = fmaf(gv, ip[(int64_t)gy * W + gx], a[k]);
+        const float v = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? ip[(int64_t)gy * W + gx] : 0.0f;
+#pragma unroll
+        for (int j = 0; j < WG_CO; ++j) a[j][c][k] = fmaf(g[j], v, a[j][c][k]);
       }
     }
   }
-  __shared__ float red[9][8];
+  // Block sums: warp shuffles, then one value per warp through shared memory.
+  constexpr int NV = WG_CO * WG_CI * 9 + WG_CO;
+  __shared__ float red[NV][8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    float v = a[k];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) red[k][warp] = v;
+  for (int v = 0; v < NV; ++v) {
+    float x = v < WG_CO * WG_CI * 9 ? a[v / (WG_CI * 9)][(v / 9) % WG_CI][v % 9] : b[v - WG_CO * WG_CI * 9];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) red[v][warp] = x;
   }
   __syncthreads();
-  if (threadIdx.x < 9) {
-    float v = 0.0f;
-    for (int j = 0; j < (int)(blockDim.x >> 5); ++j) v += red[threadIdx.x][j];
-    dw[((int64_t)co * ci_n + ci) * 9 + threadIdx.x] = v;
+  for (int v = threadIdx.x; v < NV; v += blockDim.x) {
+    float x = 0.0f;
+    for (int j = 0; j < (int)(blockDim.x >> 5); ++j) x += red[v][j];
+    if (v < WG_CO * WG_CI * 9) {
+      const int j = v / (WG_CI * 9), c = (v / 9) % WG_CI, k = v % 9;
+      if (co0 + j < co_n && ci0 + c < ci_n)
+        part[(((int64_t)s * co_n + co0 + j) * ci_n + ci0 + c) * 9 + k] = x;
+    } else if (blockIdx.x == 0) {
+      const int j = v - WG_CO * WG_CI * 9;
+      if (co0 + j < co_n) part_b[(int64_t)s * co_n + co0 + j] = x;
+    }
   }
 }
 
-__global__ void __launch_bounds__(256)
-k_bias_grad(const float* __restrict__ dout, int64_t dout_ns, int n_img, int64_t hw, float* db) {
-  const int co = blockIdx.x;
-  float a = 0.0f;
-  for (int n = 0; n < n_img; ++n)
-    for (int64_t p = threadIdx.x; p < hw; p += blockDim.x) a += dout[n * dout_ns + co * hw + p];
-  __shared__ float red[8];
-  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float v = 0.0f;
-    for (int j = 0; j < (int)(blockDim.x >> 5); ++j) v += red[j];
-    db[co] = v;
-  }
+__global__ void k_wgrad_reduce(const float* __restrict__ part, int64_t per, float* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= per) return;
+  float x = 0.0f;
+  for (int s = 0; s < kWgChunks; ++s) x += part[s * per + i];
+  out[i] = x;
 }
 
 __global__ void k_flip(const float* __restrict__ w, int co_n, int ci_n, float* __restrict__ wt) {
@@ -247,10 +268,18 @@ cudaError_t dn_conv3x3(const float* in, int64_t in_ns, int ci, float* out, int64
   return cudaGetLastError();
 }
 
+size_t dn_wgrad_scratch_floats(int co, int ci) { return (size_t)kWgChunks * ((size_t)co * ci * 9 + co); }
+
 cudaError_t dn_conv3x3_wgrad(const float* in, int64_t in_ns, int ci, const float* dout, int64_t dout_ns,
-                             int co, int n, int h, int w, float* dw, float* db, cudaStream_t s) {
-  k_conv3x3_wgrad<<<dim3(ci, co), 256, 0, s>>>(in, in_ns, ci, dout, dout_ns, n, h, w, dw);
-  if (db) k_bias_grad<<<co, 256, 0, s>>>(dout, dout_ns, n, (int64_t)h * w, db);
+                             int co, int n, int h, int w, float* dw, float* db, float* scratch,
+                             cudaStream_t s) {
+  const int64_t per_w = (int64_t)co * ci * 9;
+  float* part = scratch;
+  float* part_b = scratch + kWgChunks * per_w;
+  const dim3 grid((ci + WG_CI - 1) / WG_CI, (co + WG_CO - 1) / WG_CO, kWgChunks);
+  k_wgrad_part<<<grid, 256, 0, s>>>(in, in_ns, ci, dout, dout_ns, co, n, h, w, part, part_b);
+  k_wgrad_reduce<<<blocks_for(per_w), 256, 0, s>>>(part, per_w, dw);
+  if (db) k_wgrad_reduce<<<blocks_for(co), 256, 0, s>>>(part_b, co, db);
   return cudaGetLastError();
 }
 

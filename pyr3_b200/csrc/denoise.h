@@ -14,10 +14,13 @@ cudaError_t dn_conv3x3(const float* in, int64_t in_ns, int ci, float* out, int64
                        int n, int h, int w, const float* weight, const float* bias, bool relu,
                        cudaStream_t s);
 // dw[co, ci, k] = sum over images and pixels of dout[co] * shifted in[ci];
-// db[co] = sum of dout[co] (db may be null).  Overwrites dw / db.
+// db[co] = sum of dout[co] (db may be null).  Overwrites dw / db.  The sum
+// is split over 32 pixel chunks whose partials go to scratch
+// (dn_wgrad_scratch_floats(co, ci) floats) and are added in a fixed order.
+size_t dn_wgrad_scratch_floats(int co, int ci);
 cudaError_t dn_conv3x3_wgrad(const float* in, int64_t in_ns, int ci, const float* dout,
                              int64_t dout_ns, int co, int n, int h, int w, float* dw, float* db,
-                             cudaStream_t s);
+                             float* scratch, cudaStream_t s);
 // wt[ci][co][k] = w[co][ci][8 - k]: the data gradient of a 3x3 convolution
 // is the convolution of dout with these weights.
 cudaError_t dn_flip_weights(const float* w, int co, int ci, float* wt, cudaStream_t s);

@@ -100,6 +100,9 @@ class UNet:
         self.steps = 0
         self.launches = 0  # kernels this network has queued
         self.wt = torch.zeros(max(co * ci * 9 for co, ci in self.shapes), **f32)  # flipped weights
+        lib = _lib.lib()
+        self.wsc_n = max(lib.pyr3_dn_wgrad_scratch_floats(co, ci) for co, ci in self.shapes)
+        self.wsc = torch.zeros(self.wsc_n, **f32)  # weight-gradient partials
         hs = [(h >> l, w >> l) for l in range(L)]
         self.hs = hs
         z = lambda c, l: torch.zeros((n, c, hs[l][0], hs[l][1]), **f32)  # noqa: E731
@@ -168,11 +171,11 @@ class UNet:
                                   C.c_void_p(self.wt.data_ptr()), None, 0, self._stream()))
 
     def _wgrad(self, src, ci, g, co, l, i):
-        self.launches += 2
+        self.launches += 3
         dw, db = self._gw(i)
         h, wd = self.hs[l]
         _check(_lib.lib().pyr3_dn_conv3x3_wgrad(src[0], src[1], ci, g[0], g[1], co, self.n, h, wd, dw, db,
-                                                self._stream()))
+                                                C.c_void_p(self.wsc.data_ptr()), self.wsc_n, self._stream()))
 
     def _mask(self, g, y, c, l):
         self.launches += 1
@@ -264,6 +267,32 @@ class UNet:
                 _check(lib.pyr3_dn_pool2(gi[0], gi[1], dst[0], dst[1], ch[l - 1], self.n, h[0], h[1], 1, 1, st()))
                 self.launches += 1
 
+    def capture(self) -> None:
+        """Record forward, loss and backward as one CUDA graph, so that a
+        training step is one graph launch plus the Adam kernel instead of
+        ~130 separate launches from Python.  Every captured kernel is this
+        library's; replay() reruns them on whatever x and tgt hold."""
+        t = self.t
+        side = t.cuda.Stream(self.dev)
+        side.wait_stream(t.cuda.current_stream(self.dev))
+        with t.cuda.stream(side):  # every kernel runs once before capture
+            self.forward()
+            self.loss_and_grad()
+            self.backward()
+        t.cuda.current_stream(self.dev).wait_stream(side)
+        self.graph = t.cuda.CUDAGraph()
+        n0 = self.launches
+        with t.cuda.graph(self.graph):
+            self.forward()
+            self.loss_and_grad()
+            self.backward()
+        self.graph_launches = self.launches - n0
+
+    def replay(self) -> None:
+        """forward + loss_and_grad + backward from the captured graph."""
+        self.graph.replay()
+        self.launches += self.graph_launches
+
     def step(self, lr: float = 1e-3, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8) -> None:
         self.steps += 1
         self.launches += 1
@@ -348,6 +377,8 @@ def train(xs, ts, steps: int = 300, batch: int = 8, crop: int = 128, lr: float =
     T = torch.tensor(ts, device=dev)
     n, _, H, W = xs.shape
     net = UNet(batch, crop, crop, init_params(chans, seed) if params is None else params, chans=chans)
+    net.capture()
+    net.launches = 0
     losses = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -357,9 +388,7 @@ def train(xs, ts, steps: int = 300, batch: int = 8, crop: int = 128, lr: float =
         for j in range(batch):
             net.x[j].copy_(X[idx[j], :, ys[j]:ys[j] + crop, xo[j]:xo[j] + crop])
             net.tgt[j].copy_(T[idx[j], :, ys[j]:ys[j] + crop, xo[j]:xo[j] + crop])
-        net.forward()
-        net.loss_and_grad()
-        net.backward()
+        net.replay()
         net.step(lr=lr)
         if s % 25 == 0 or s == steps - 1:
             losses.append((s, net.read_loss()))

@@ -15,7 +15,7 @@ HDR = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "pyr3.
 
 
 def test_library_exports_every_header_symbol():
-    names = set(re.findall(r"^\s*(?:int|const char \*)\s*\*?\s*(pyr3_\w+)\s*\(", open(HDR).read(), re.M))
+    names = set(re.findall(r"^\s*(?:int|uint64_t|const char \*)\s*\*?\s*(pyr3_\w+)\s*\(", open(HDR).read(), re.M))
     assert len(names) >= 25
     L = _lib.lib()
     missing = [n for n in sorted(names) if not hasattr(L, n)]

@@ -129,8 +129,15 @@ def test_cuda_layers_match_oracle():
     _close(yd, D.conv3x3(x, wt, b, relu=True))
     dw = torch.zeros_like(wd)
     db = torch.zeros_like(bd)
+    nsc = L.pyr3_dn_wgrad_scratch_floats(co, ci)
+    sc = torch.zeros(nsc, device="cuda")
+    with pytest.raises(Exception):  # too little scratch is refused
+        ck(L.pyr3_dn_conv3x3_wgrad(_p(xd), ci * h * w, ci, _p(gd), co * h * w, co, n, h, w,
+                                   C.c_void_p(dw.data_ptr()), C.c_void_p(db.data_ptr()), C.c_void_p(sc.data_ptr()),
+                                   nsc - 1, None))
     ck(L.pyr3_dn_conv3x3_wgrad(_p(xd), ci * h * w, ci, _p(gd), co * h * w, co, n, h, w,
-                               C.c_void_p(dw.data_ptr()), C.c_void_p(db.data_ptr()), None))
+                               C.c_void_p(dw.data_ptr()), C.c_void_p(db.data_ptr()), C.c_void_p(sc.data_ptr()),
+                               nsc, None))
     ref_dw, ref_db = D.conv3x3_wgrad(x, g)
     torch.cuda.synchronize()
     _close(dw, ref_dw, rtol=1e-4, atol=1e-3)
@@ -210,6 +217,12 @@ def test_cuda_unet_forward_backward_matches_oracle():
     got = net.grads().astype(np.float64)
     scale = np.abs(grad).max()
     assert float(np.abs(got - grad).max()) <= 1e-3 * scale, float(np.abs(got - grad).max() / scale)
+    # the captured graph reruns the same kernels: the same gradient, bit for bit
+    net.capture()
+    net.g.zero_()
+    net.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(net.grads(), got.astype(np.float32))
 
 
 @pytest.mark.gpu
