@@ -439,7 +439,7 @@ def bench_reference(args, ws, rank, local, dist):
 
 
 def bench_denoise(args, ws, rank, local, dist):
-    """Learned denoiser: a step = 50 Adam steps on batches of 8 random
+    """Learned denoiser: a step = 200 Adam steps on batches of 8 random
     128x128 crops from 64 training genomes' (25 spp features, 2000 spp
     target) renders at 256x256; afterwards the 8 held-out genomes are
     denoised and scored (PSNR against their 2000-spp renders)."""
@@ -455,7 +455,7 @@ def bench_denoise(args, ws, rank, local, dist):
     xs, ts = DN.make_dataset(gs)
     render_s = _t.perf_counter() - t0
     xtr, ttr, xho, tho = xs[:64], ts[:64], xs[64:], ts[64:]
-    per = 50
+    per = 200
     batch, crop = 8, 128
     net, _, _ = DN.train(xtr, ttr, steps=per * args.warmup, batch=batch, crop=crop, seed=1)
     params = net.params()
