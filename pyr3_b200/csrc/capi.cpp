@@ -795,8 +795,8 @@ PYR3_API int pyr3_last_iterate_ms(pyr3_renderer* r, float* ms) {
 // iterations per walker to keep the 200-iteration burn-in under ~10 %,
 // since the GPU is filled by running many genomes at once.
 //
-// Genomes large enough to fill the GPU on their own (at least the
-// autotuner's 2^26 samples, pooled walkers) stay out of the graph: each
+// Genomes large enough to fill the GPU on their own (at least
+// kBatchSoloSamples, pooled walkers) stay out of the graph: each
 // runs through pyr3_iterate on its autotuned kernel, one after another on
 // their renderers' streams, while the graph runs the small ones.  Their
 // genome records are copied at creation.  Graph genomes use module
@@ -822,6 +822,9 @@ struct pyr3_batch {
 
 namespace {
 constexpr uint64_t kBatchItersPerWalker = 2000;
+// Measured on the 256-genome batch: run alone, one after another, every
+// genome of 2^24 samples or more beats sharing the GPU with the graph.
+constexpr uint64_t kBatchSoloSamples = 1ull << 24;
 
 void free_batch(pyr3_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -879,7 +882,7 @@ PYR3_API int pyr3_batch_create(pyr3_renderer* const* renderers, const pyr3_genom
     if (!e.empty())
       return fail(e.find("not implemented") != std::string::npos ? PYR3_E_UNSUPPORTED : PYR3_E_INVALID, e);
     const uint64_t total = o->walkers * o->iters_per_walker;
-    if (!(o->flags & PYR3_ITER_EXACT_WALKERS) && total >= kTuneMinSamples) {
+    if (!(o->flags & PYR3_ITER_EXACT_WALKERS) && total >= kBatchSoloSamples) {
       const size_t nrec = (size_t)g->n_xforms + (g->final_slot >= 0 ? 1 : 0);
       b->solo_xf.emplace_back(g->xforms, g->xforms + nrec * 116);
       b->solo_xaos.emplace_back();

@@ -2,7 +2,7 @@
 the same genome rendered alone through the per-genome path -- statistically,
 since walker counts and seeds differ -- and gets exactly its samples.  Two
 genomes of the batch share a structure, so each needs its own module
-instance; the last genome is large enough (>= 2^26 samples) to run beside
+instance; the last genome is large enough (>= 2^24 samples) to run beside
 the graph through the per-genome path, on a structure the graph also uses."""
 import copy
 
@@ -33,8 +33,8 @@ def _genomes():
         g.oversample = 1
         g.density = None
         g.scale = W / 4
-        g.quality = 2560.0  # 4.9e7 samples each
-    big.quality = 3600.0  # 6.9e7 samples: outside the graph
+        g.quality = 640.0  # 1.2e7 samples each: in the graph
+    big.quality = 3600.0  # 6.9e7 samples: beside the graph
     return gs
 
 
