@@ -92,12 +92,22 @@ def build(force: bool = False) -> str:
     cmd = [NVCC, "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
            "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared",
            "-I", os.path.join(ROOT, "include"), "-I", CSRC, *srcs, "-o", LIB,
-           "-cudart", "static", "-L", CUDA_LIB, "-lnvrtc",
+           "-cudart", "static", "-L", CUDA_LIB, "-lnvrtc", "-ldl",
            "-Xlinker", f"-rpath,{CUDA_LIB}"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
     return LIB
+
+
+CUBINS = os.path.join(PKG, "_cubins")
+
+
+def make_cubin_cache() -> str:
+    """The in-package cubin cache the library uses when PYR3_CACHE_DIR is
+    unset (filled by tests/precompile_modules.py)."""
+    os.makedirs(CUBINS, exist_ok=True)
+    return CUBINS
 
 
 if __name__ == "__main__":

@@ -3,6 +3,7 @@
 // by a hash of the generated source.
 #include "jit.h"
 
+#include <dlfcn.h>
 #include <nvrtc.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -35,11 +36,21 @@ uint64_t fnv1a(const std::string& s) {
   return h;
 }
 
+// Cubin cache: $PYR3_CACHE_DIR; else a `_cubins` directory beside this
+// shared library, if one exists (the build fills it, so a copy of the
+// package carries its compiled modules); else ~/.cache/pyr3_b200.
 std::string cache_dir() {
   const char* d = std::getenv("PYR3_CACHE_DIR");
   std::string dir;
+  Dl_info info;
+  struct stat st;
   if (d && *d) {
     dir = d;
+  } else if (dladdr((void*)&cache_dir, &info) && info.dli_fname &&
+             std::strrchr(info.dli_fname, '/') &&
+             stat((std::string(info.dli_fname, std::strrchr(info.dli_fname, '/')) + "/_cubins").c_str(), &st) == 0 &&
+             S_ISDIR(st.st_mode)) {
+    dir = std::string(info.dli_fname, std::strrchr(info.dli_fname, '/')) + "/_cubins";
   } else {
     const char* home = std::getenv("HOME");
     dir = std::string(home && *home ? home : "/tmp") + "/.cache/pyr3_b200";
