@@ -522,8 +522,10 @@ def bench_denoise(args, ws, rank, local, dist):
                 "h2d_bytes_per_step": int(hx.nbytes + ht.nbytes) * per, "d2h_bytes_per_step": 4 * per},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None,
-                     "note": f"FLOPs = 3 x 2 x sum(ci co 9 H_l W_l) per pixel = {flop_pix:.0f}; the layers run "
-                             f"in f32 on the CUDA cores (no tensor-core path yet); peak = bf16 dense, {pk}"},
+                     "note": f"FLOPs = 3 x 2 x sum(ci co 9 H_l W_l) per pixel = {flop_pix:.0f}; forward and "
+                             f"data-gradient convolutions on tcgen05 (bf16 operands, f32 accumulation), weight "
+                             f"gradients in f32 on the CUDA cores; im2col staging from NCHW f32 bounds the "
+                             f"tensor-core kernel; peak = bf16 dense, {pk}"},
         "gpu_launches": launches,
         "clocks": clk,
     }

@@ -264,6 +264,11 @@ int pyr3_prepare(pyr3_renderer *r, const pyr3_genome *g);
 int pyr3_dn_conv3x3(const float *in, int64_t in_ns, int32_t ci, float *out, int64_t out_ns,
                     int32_t co, int32_t n, int32_t h, int32_t w, const float *weight,
                     const float *bias, int32_t relu, void *stream);
+/* pyr3_dn_conv3x3 on the tensor cores (tcgen05): input and weights rounded
+ * to bf16, products accumulated in f32; co <= 128 (PYR3_E_INVALID above). */
+int pyr3_dn_conv3x3_bf16(const float *in, int64_t in_ns, int32_t ci, float *out, int64_t out_ns,
+                         int32_t co, int32_t n, int32_t h, int32_t w, const float *weight,
+                         const float *bias, int32_t relu, void *stream);
 /* Weight (and, if dbias is not NULL, bias) gradient of pyr3_dn_conv3x3
  * given its input and the gradient of its output; overwrites.  The sum
  * over pixels is split into partials held in `scratch`, a device buffer

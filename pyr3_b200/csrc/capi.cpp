@@ -1022,6 +1022,16 @@ PYR3_API int pyr3_dn_conv3x3(const float* in, int64_t in_ns, int32_t ci, float* 
   return PYR3_OK;
 }
 
+PYR3_API int pyr3_dn_conv3x3_bf16(const float* in, int64_t in_ns, int32_t ci, float* out, int64_t out_ns,
+                                  int32_t co, int32_t n, int32_t h, int32_t w, const float* weight,
+                                  const float* bias, int32_t relu, void* stream) {
+  if (!in || !out || !weight || !dn_dims_ok(ci, co, n, (int64_t)h * w) || h <= 0 || w <= 0 || co > 128)
+    return fail(PYR3_E_INVALID, "conv3x3_bf16: null operand, non-positive size or more than 128 outputs");
+  CUDA_TRY(pyr3::dn_conv3x3_bf16(in, in_ns, ci, out, out_ns, co, n, h, w, weight, bias, relu != 0,
+                                 (cudaStream_t)stream));
+  return PYR3_OK;
+}
+
 PYR3_API int pyr3_dn_conv3x3_wgrad(const float* in, int64_t in_ns, int32_t ci, const float* dout,
                                    int64_t dout_ns, int32_t co, int32_t n, int32_t h, int32_t w,
                                    float* dweight, float* dbias, float* scratch, uint64_t scratch_floats,

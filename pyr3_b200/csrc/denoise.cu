@@ -4,6 +4,8 @@
 // accumulates 8 output channels of one pixel.
 #include "denoise.h"
 
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cmath>
 
@@ -259,6 +261,150 @@ __global__ void k_adam(float* p, const float* __restrict__ g, float* m, float* v
 
 unsigned blocks_for(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
 
+// ---- 3x3 convolution on the tensor cores (tcgen05, bf16 x bf16 -> f32)
+// Implicit GEMM: D[pixel][co] = sum_k A[pixel][k] * B[co][k], k = ci * 9 +
+// ky * 3 + kx, over a CTA tile of 16 x 8 output pixels (M = 128) and all
+// output channels (N = NP, padded to a multiple of 16).  K is staged in
+// chunks of 64: the 128 threads gather the chunk's im2col rows and weights,
+// rounded to bf16, into shared memory in the no-swizzle K-major canonical
+// layout (8 x 8-element core matrices: 128 B apart along K, 256 B apart
+// along M / N); one thread issues the four K = 16 MMAs and commits them to
+// an mbarrier that every thread waits on (bounded) before the chunk's
+// buffers are refilled.  The accumulator lives in TMEM; each warp reads its
+// 32 rows back with tcgen05.ld, adds the bias, applies ReLU and stores f32.
+constexpr int TC_TX = 16, TC_TY = 8, TC_KC = 64;
+constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  // start >> 4, LBO 128 B >> 4, SBO 256 B >> 4, descriptor version 1, no swizzle
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(256u >> 4) << 32) |
+         ((uint64_t)1 << 46);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+template <int NP>
+__global__ void __launch_bounds__(128)
+k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __restrict__ out, int64_t out_ns,
+             int co_n, int H, int W, const float* __restrict__ wt, const float* __restrict__ bias, int relu) {
+  constexpr uint32_t NCOL = NP <= 32 ? 32 : (NP <= 64 ? 64 : 128);
+  extern __shared__ __align__(1024) unsigned char smem[];
+  // per K step of 16: A = 16 row groups x 2 core matrices x 8 rows of 16 B
+  // (256 x 16 B), B = NP / 8 row groups x 2 x 8 rows (2 NP x 16 B)
+  uint4* sa = reinterpret_cast<uint4*>(smem);
+  uint4* sb = sa + 4 * 128 * 2;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int x0 = blockIdx.x * TC_TX, y0 = blockIdx.y * TC_TY, n = blockIdx.z;
+  const int K = ci_n * 9, nchunks = (K + TC_KC - 1) / TC_KC;
+  const int64_t hw = (int64_t)H * W;
+  const float* inn = in + n * in_ns;
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n"
+                 "fence.mbarrier_init.release.cluster;" ::"r"(smem_addr(&bar)) : "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base)),
+                 "r"(NCOL) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NP >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  // this thread's pixel (row of A)
+  const int py = y0 + t / TC_TX, px = x0 + t % TC_TX;
+  for (int c = 0; c < nchunks; ++c) {
+    const int k0 = c * TC_KC;
+    // A: 8 groups of 8 consecutive k for pixel t, one 16-byte store each
+#pragma unroll 1
+    for (int g = 0; g < TC_KC / 8; ++g) {
+      float v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int k = k0 + g * 8 + j;
+        float x = 0.0f;
+        if (k < K) {
+          const int ci = k / 9, tap = k - ci * 9;
+          const int yy = py + tap / 3 - 1, xx = px + tap % 3 - 1;
+          if (yy >= 0 && yy < H && xx >= 0 && xx < W) x = inn[ci * hw + (int64_t)yy * W + xx];
+        }
+        v[j] = x;
+      }
+      const int s = g >> 1, h = g & 1;
+      sa[(s * 32 + (t >> 3) * 2 + h) * 8 + (t & 7)] =
+          make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
+    }
+    // B: NP rows x 8 groups
+    for (int idx = t; idx < NP * (TC_KC / 8); idx += 128) {
+      const int co = idx >> 3, g = idx & 7;
+      float v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int k = k0 + g * 8 + j;
+        v[j] = (co < co_n && k < K) ? wt[(int64_t)co * K + k] : 0.0f;
+      }
+      const int s = g >> 1, h = g & 1;
+      sb[(s * (NP / 4) + (co >> 3) * 2 + h) * 8 + (co & 7)] =
+          make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int s = 0; s < 4; ++s) {
+        const uint64_t da = umma_desc(smem_addr(sa + (size_t)s * 128 * 2));
+        const uint64_t db = umma_desc(smem_addr(sb + (size_t)s * NP * 2));
+        const uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
+        asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                     ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   ::"r"(smem_addr(&bar)) : "memory");
+    }
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < TC_WAIT_LIMIT && !done; ++it)
+      asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                   : "=r"(done) : "r"(smem_addr(&bar)), "r"((uint32_t)(c & 1)) : "memory");
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  // epilogue: rows warp*32 + lane of TMEM, 8 columns at a time
+  const int r = warp * 32 + lane;
+  const int oy = y0 + r / TC_TX, ox = x0 + r % TC_TX;
+  const bool inside = oy < H && ox < W;
+#pragma unroll 1
+  for (int c0 = 0; c0 < NP; c0 += 8) {
+    uint32_t v[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (inside) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int co = c0 + j;
+        if (co < co_n) {
+          float x = __uint_as_float(v[j]) + (bias ? bias[co] : 0.0f);
+          if (relu) x = fmaxf(x, 0.0f);
+          out[n * out_ns + co * hw + (int64_t)oy * W + ox] = x;
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL) : "memory");
+}
+
 }  // namespace
 
 cudaError_t dn_conv3x3(const float* in, int64_t in_ns, int ci, float* out, int64_t out_ns, int co, int n,
@@ -269,6 +415,31 @@ cudaError_t dn_conv3x3(const float* in, int64_t in_ns, int ci, float* out, int64
 }
 
 size_t dn_wgrad_scratch_floats(int co, int ci) { return (size_t)kWgChunks * ((size_t)co * ci * 9 + co); }
+
+template <int NP>
+cudaError_t launch_tc(const float* in, int64_t in_ns, int ci, float* out, int64_t out_ns, int co, int n, int h,
+                      int w, const float* weight, const float* bias, bool relu, cudaStream_t s) {
+  const size_t smem = (size_t)(4 * 128 * 2 + 4 * NP * 2) * 16;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_conv3x3_tc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  const dim3 grid((w + TC_TX - 1) / TC_TX, (h + TC_TY - 1) / TC_TY, n);
+  k_conv3x3_tc<NP><<<grid, 128, smem, s>>>(in, in_ns, ci, out, out_ns, co, h, w, weight, bias, relu ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_conv3x3_bf16(const float* in, int64_t in_ns, int ci, float* out, int64_t out_ns, int co, int n,
+                            int h, int w, const float* weight, const float* bias, bool relu, cudaStream_t s) {
+  if (co <= 16) return launch_tc<16>(in, in_ns, ci, out, out_ns, co, n, h, w, weight, bias, relu, s);
+  if (co <= 32) return launch_tc<32>(in, in_ns, ci, out, out_ns, co, n, h, w, weight, bias, relu, s);
+  if (co <= 48) return launch_tc<48>(in, in_ns, ci, out, out_ns, co, n, h, w, weight, bias, relu, s);
+  if (co <= 64) return launch_tc<64>(in, in_ns, ci, out, out_ns, co, n, h, w, weight, bias, relu, s);
+  if (co <= 96) return launch_tc<96>(in, in_ns, ci, out, out_ns, co, n, h, w, weight, bias, relu, s);
+  if (co <= 128) return launch_tc<128>(in, in_ns, ci, out, out_ns, co, n, h, w, weight, bias, relu, s);
+  return cudaErrorInvalidValue;
+}
 
 cudaError_t dn_conv3x3_wgrad(const float* in, int64_t in_ns, int ci, const float* dout, int64_t dout_ns,
                              int co, int n, int h, int w, float* dw, float* db, float* scratch,

@@ -13,6 +13,11 @@ namespace pyr3 {
 cudaError_t dn_conv3x3(const float* in, int64_t in_ns, int ci, float* out, int64_t out_ns, int co,
                        int n, int h, int w, const float* weight, const float* bias, bool relu,
                        cudaStream_t s);
+// The same convolution on the tensor cores (tcgen05): inputs and weights
+// rounded to bf16, f32 accumulation; co <= 128.
+cudaError_t dn_conv3x3_bf16(const float* in, int64_t in_ns, int ci, float* out, int64_t out_ns, int co,
+                            int n, int h, int w, const float* weight, const float* bias, bool relu,
+                            cudaStream_t s);
 // dw[co, ci, k] = sum over images and pixels of dout[co] * shifted in[ci];
 // db[co] = sum of dout[co] (db may be null).  Overwrites dw / db.  The sum
 // is split over 32 pixel chunks whose partials go to scratch

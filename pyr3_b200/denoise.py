@@ -1,6 +1,8 @@
 """Learned denoiser: a small U-Net that maps a low-sample render (8 feature
 channels) to the colours of a high-sample render of the same genome,
-trained and run with this library's CUDA layers (pyr3_dn_* in the C-ABI).
+trained and run with this library's CUDA layers (pyr3_dn_* in the C-ABI):
+the forward and data-gradient convolutions on the tensor cores (tcgen05,
+bf16 operands, f32 accumulation) by default, or all in f32.
 The denoiser has no counterpart in the reference.
 
 PyTorch only allocates device memory and supplies the stream here; every
@@ -72,7 +74,8 @@ class UNet:
     of 2^(levels-1)).  forward() then backward() computes the parameter
     gradient of the MSE against a target; step() applies Adam."""
 
-    def __init__(self, n: int, h: int, w: int, params: np.ndarray, chans=CHANS, device: int = 0):
+    def __init__(self, n: int, h: int, w: int, params: np.ndarray, chans=CHANS, device: int = 0,
+                 tensor_cores: bool = True):
         import torch
 
         if not torch.cuda.is_available():
@@ -81,6 +84,7 @@ class UNet:
         if h % (1 << (L - 1)) or w % (1 << (L - 1)):
             raise ValueError(f"H and W must be multiples of {1 << (L - 1)}")
         self.t = torch
+        self.tc = tensor_cores  # forward and data-gradient convolutions on tcgen05 (bf16 operands)
         self.dev = torch.device("cuda", device)
         self.n, self.h, self.w, self.chans = n, h, w, tuple(chans)
         self.L = L
@@ -157,8 +161,9 @@ class UNet:
         self.launches += 1
         w, b = self._w(i)
         h, wd = self.hs[l]
-        _check(_lib.lib().pyr3_dn_conv3x3(src[0], src[1], ci, dst[0], dst[1], co, self.n, h, wd, w,
-                                          b if bias else None, 1 if relu else 0, self._stream()))
+        fn = _lib.lib().pyr3_dn_conv3x3_bf16 if self.tc else _lib.lib().pyr3_dn_conv3x3
+        _check(fn(src[0], src[1], ci, dst[0], dst[1], co, self.n, h, wd, w, b if bias else None,
+                  1 if relu else 0, self._stream()))
 
     def _dgrad(self, g, co, dst, ci, l, i):
         """dst = input gradient of conv i (co <- ci) from its output gradient g."""
@@ -167,8 +172,9 @@ class UNet:
         L_ = _lib.lib()
         _check(L_.pyr3_dn_flip_weights(w, co, ci, C.c_void_p(self.wt.data_ptr()), self._stream()))
         h, wd = self.hs[l]
-        _check(L_.pyr3_dn_conv3x3(g[0], g[1], co, dst[0], dst[1], ci, self.n, h, wd,
-                                  C.c_void_p(self.wt.data_ptr()), None, 0, self._stream()))
+        fn = L_.pyr3_dn_conv3x3_bf16 if self.tc else L_.pyr3_dn_conv3x3
+        _check(fn(g[0], g[1], co, dst[0], dst[1], ci, self.n, h, wd, C.c_void_p(self.wt.data_ptr()), None, 0,
+                  self._stream()))
 
     def _wgrad(self, src, ci, g, co, l, i):
         self.launches += 3
@@ -397,11 +403,11 @@ def train(xs, ts, steps: int = 300, batch: int = 8, crop: int = 128, lr: float =
     return net, losses, e0.elapsed_time(e1)
 
 
-def evaluate(params, xs, ts, chans=CHANS):
+def evaluate(params, xs, ts, chans=CHANS, tensor_cores: bool = True):
     """(PSNR of the noisy input, PSNR of the denoised output) against the
     targets, over all images, and the denoised images."""
     n, _, H, W = xs.shape
-    net = UNet(n, H, W, params, chans=chans)
+    net = UNet(n, H, W, params, chans=chans, tensor_cores=tensor_cores)
     net.set_batch(xs, ts)
     net.forward()
     out = np.clip(net.output(), 0.0, 1.0)

@@ -103,6 +103,13 @@ def _p(t, c0=0):
     return C.c_void_p(t.data_ptr() + 4 * c0 * t.shape[2] * t.shape[3])
 
 
+def _bf16(a):
+    """f32 rounded to bf16 (nearest even), as float64."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
 def _close(got, want, rtol=2e-4, atol=2e-5):
     got = got.detach().cpu().numpy().astype(np.float64) if isinstance(got, torch.Tensor) else got
     err = np.abs(got - want) - (atol + rtol * np.abs(want))
@@ -149,6 +156,17 @@ def test_cuda_layers_match_oracle():
                          None, 0, None))
     torch.cuda.synchronize()
     _close(dx, D.conv3x3_dgrad(g, wt))
+    # tensor-core convolution: the oracle on bf16-rounded operands, f32 sums
+    for co2 in (co, 40, 90):
+        w2 = rng.normal(size=(co2, ci, 3, 3)) * 0.2
+        b2 = rng.normal(size=co2)
+        w2d, b2d = _dev(w2), _dev(b2)
+        y2 = torch.zeros((n, co2, h, w), device="cuda")
+        ck(L.pyr3_dn_conv3x3_bf16(_p(xd), ci * h * w, ci, _p(y2), co2 * h * w, co2, n, h, w,
+                                  C.c_void_p(w2d.data_ptr()), C.c_void_p(b2d.data_ptr()), 1, None))
+        torch.cuda.synchronize()
+        want = D.conv3x3(_bf16(x), _bf16(w2), b2.astype(np.float32).astype(np.float64), relu=True)
+        _close(y2, want, rtol=1e-4, atol=1e-4)
     # pool / upsample on a channel slice of a wider tensor (stride != channels * hw)
     big = _dev(rng.normal(size=(n, 7, h, w)))
     src = big.cpu().numpy().astype(np.float64)[:, 2:5]
@@ -203,7 +221,7 @@ def test_cuda_unet_forward_backward_matches_oracle():
     n, h, w = 2, 32, 48
     x = rng.normal(size=(n, 8, h, w))
     tgt = rng.normal(size=(n, 3, h, w))
-    net = DN.UNet(n, h, w, params, chans=chans)
+    net = DN.UNet(n, h, w, params, chans=chans, tensor_cores=False)
     net.set_batch(x, tgt)
     net.forward()
     net.loss_and_grad()
@@ -223,6 +241,18 @@ def test_cuda_unet_forward_backward_matches_oracle():
     net.replay()
     torch.cuda.synchronize()
     assert np.array_equal(net.grads(), got.astype(np.float32))
+    # the tensor-core network (bf16 operands, f32 accumulation) stays close
+    tcn = DN.UNet(n, h, w, params, chans=chans, tensor_cores=True)
+    tcn.set_batch(x, tgt)
+    tcn.forward()
+    tcn.loss_and_grad()
+    tcn.backward()
+    torch.cuda.synchronize()
+    o2 = tcn.output().astype(np.float64)
+    assert float(np.abs(o2 - out).max()) <= 3e-2 * float(np.abs(out).max())
+    g2 = tcn.grads().astype(np.float64)
+    cos = float(g2 @ grad / (np.linalg.norm(g2) * np.linalg.norm(grad)))
+    assert cos >= 0.99, cos
 
 
 @pytest.mark.gpu
