@@ -262,30 +262,42 @@ __global__ void k_adam(float* p, const float* __restrict__ g, float* m, float* v
 unsigned blocks_for(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
 
 // ---- 3x3 convolution on the tensor cores (tcgen05, bf16 x bf16 -> f32)
-// Implicit GEMM: D[pixel][co] = sum_k A[pixel][k] * B[co][k], k = ci * 9 +
-// ky * 3 + kx, over a CTA tile of 16 x 8 output pixels (M = 128) and all
-// output channels (N = NP, padded to a multiple of 16).  K is staged in
-// chunks of 64: the 128 threads gather the chunk's im2col rows and weights,
-// rounded to bf16, into shared memory in the no-swizzle K-major canonical
-// layout (8 x 8-element core matrices: 128 B apart along K, 256 B apart
-// along M / N); one thread issues the four K = 16 MMAs and commits them to
-// an mbarrier that every thread waits on (bounded) before the chunk's
-// buffers are refilled.  The accumulator lives in TMEM; each warp reads its
-// 32 rows back with tcgen05.ld, adds the bias, applies ReLU and stores f32.
-constexpr int TC_TX = 16, TC_TY = 8, TC_KC = 64;
+// Implicit GEMM without im2col.  Index the zero-padded input by position
+// q = (y + 1) * P + (x + 1), P = W + 2: output q reads input q + d for tap
+// (ky, kx), d = (ky - 1) * P + (kx - 1) -- the same shift for every pixel.
+// A CTA owns 128 consecutive output positions (M = 128; positions in the
+// padding columns are computed and dropped) and stages the padded input
+// rows it needs, R = 128 + 2 (P + 1), once: plane g holds channels 8g..8g+7
+// as one 16-byte bf16 row per position, so the operand of tap t and K step
+// s (channels 16s..16s+15) is planes 2s and 2s+1 read from row P + 1 + d_t:
+// a no-swizzle K-major descriptor with contiguous rows (SBO = 16 B x 8) and
+// the next plane at LBO = 16 R bytes.  Per tap the weights (all output
+// channels, N = NP padded to 16) are staged in the usual canonical layout,
+// one thread issues the tap's MMAs into the TMEM accumulator and commits
+// them to an mbarrier that every thread waits on (bounded) before the
+// weights are refilled.  Each warp reads its 32 rows back (tcgen05.ld),
+// adds the bias, applies ReLU and stores the interior pixels in f32.
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;
+constexpr int TC_MAX_SMEM = 200 * 1024;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-  // start >> 4, LBO 128 B >> 4, SBO 256 B >> 4, descriptor version 1, no swizzle
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(256u >> 4) << 32) |
-         ((uint64_t)1 << 46);
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  // start >> 4, leading / stride byte offsets >> 4, descriptor version 1, no swizzle
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
   return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// Dynamic shared memory of the tensor-core convolution (bytes).
+__host__ __device__ inline size_t tc_smem_bytes(int ci, int w, int np) {
+  const size_t R = 128 + 2 * (size_t)(w + 3);
+  const size_t G = 2 * (size_t)((ci + 15) / 16);
+  return G * R * 16 + (G / 2) * (size_t)np * 32;
 }
 
 template <int NP>
@@ -294,15 +306,15 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
              int co_n, int H, int W, const float* __restrict__ wt, const float* __restrict__ bias, int relu) {
   constexpr uint32_t NCOL = NP <= 32 ? 32 : (NP <= 64 ? 64 : 128);
   extern __shared__ __align__(1024) unsigned char smem[];
-  // per K step of 16: A = 16 row groups x 2 core matrices x 8 rows of 16 B
-  // (256 x 16 B), B = NP / 8 row groups x 2 x 8 rows (2 NP x 16 B)
-  uint4* sa = reinterpret_cast<uint4*>(smem);
-  uint4* sb = sa + 4 * 128 * 2;
+  const int P = W + 2, R = 128 + 2 * (P + 1), G = 2 * ((ci_n + 15) / 16), S = G / 2;
+  uint4* sa = reinterpret_cast<uint4*>(smem);  // G planes x R rows of 16 B
+  uint4* sb = sa + (size_t)G * R;               // S K steps x (NP / 8) x 2 core matrices x 8 rows
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_base;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const int x0 = blockIdx.x * TC_TX, y0 = blockIdx.y * TC_TY, n = blockIdx.z;
-  const int K = ci_n * 9, nchunks = (K + TC_KC - 1) / TC_KC;
+  const int n = blockIdx.y;
+  const int q0 = P + 1 + blockIdx.x * 128;  // first output position of the tile
+  const int qa = q0 - (P + 1);              // position of staged row 0
   const int64_t hw = (int64_t)H * W;
   const float* inn = in + n * in_ns;
   if (t == 0) {
@@ -314,44 +326,37 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
                  "r"(NCOL) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
+  // padded input rows: plane g, row r = position qa + r, 8 channels as bf16
+  for (int i = t; i < G * R; i += 128) {
+    const int g = i / R, r = i - g * R;
+    const int q = qa + r, yy = q / P - 1, xx = q % P - 1;
+    float v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = 0.0f;
+    if (yy >= 0 && yy < H && xx >= 0 && xx < W) {
+      const float* ip = inn + (int64_t)yy * W + xx;
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (g * 8 + j < ci_n) v[j] = ip[(int64_t)(g * 8 + j) * hw];
+    }
+    sa[i] = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NP >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-  // this thread's pixel (row of A)
-  const int py = y0 + t / TC_TX, px = x0 + t % TC_TX;
-  for (int c = 0; c < nchunks; ++c) {
-    const int k0 = c * TC_KC;
-    // A: 8 groups of 8 consecutive k for pixel t, one 16-byte store each
-#pragma unroll 1
-    for (int g = 0; g < TC_KC / 8; ++g) {
+  const uint32_t lbo_a = (uint32_t)R * 16u;
+  for (int tap = 0; tap < 9; ++tap) {
+    // weights of this tap: B[co][16 s + kk] = w[co][16 s + kk][tap]
+    for (int idx = t; idx < S * NP * 2; idx += 128) {
+      const int s = idx / (NP * 2), rem = idx - s * NP * 2, co = rem >> 1, h = rem & 1;
       float v[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const int k = k0 + g * 8 + j;
-        float x = 0.0f;
-        if (k < K) {
-          const int ci = k / 9, tap = k - ci * 9;
-          const int yy = py + tap / 3 - 1, xx = px + tap % 3 - 1;
-          if (yy >= 0 && yy < H && xx >= 0 && xx < W) x = inn[ci * hw + (int64_t)yy * W + xx];
-        }
-        v[j] = x;
+        const int ci = s * 16 + h * 8 + j;
+        v[j] = (co < co_n && ci < ci_n) ? wt[((int64_t)co * ci_n + ci) * 9 + tap] : 0.0f;
       }
-      const int s = g >> 1, h = g & 1;
-      sa[(s * 32 + (t >> 3) * 2 + h) * 8 + (t & 7)] =
-          make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
-    }
-    // B: NP rows x 8 groups
-    for (int idx = t; idx < NP * (TC_KC / 8); idx += 128) {
-      const int co = idx >> 3, g = idx & 7;
-      float v[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int k = k0 + g * 8 + j;
-        v[j] = (co < co_n && k < K) ? wt[(int64_t)co * K + k] : 0.0f;
-      }
-      const int s = g >> 1, h = g & 1;
       sb[(s * (NP / 4) + (co >> 3) * 2 + h) * 8 + (co & 7)] =
           make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
     }
@@ -359,10 +364,11 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
     __syncthreads();
     if (t == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      for (int s = 0; s < 4; ++s) {
-        const uint64_t da = umma_desc(smem_addr(sa + (size_t)s * 128 * 2));
-        const uint64_t db = umma_desc(smem_addr(sb + (size_t)s * NP * 2));
-        const uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
+      const int row0 = (P + 1) + (tap / 3 - 1) * P + (tap % 3 - 1);
+      for (int s = 0; s < S; ++s) {
+        const uint64_t da = umma_desc(smem_addr(sa + (size_t)(2 * s) * R + row0), lbo_a, 128u);
+        const uint64_t db = umma_desc(smem_addr(sb + (size_t)s * NP * 2), 128u, 256u);
+        const uint32_t acc = (tap > 0 || s > 0) ? 1u : 0u;
         asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
                      ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
@@ -373,13 +379,12 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
     uint32_t done = 0;
     for (uint32_t it = 0; it < TC_WAIT_LIMIT && !done; ++it)
       asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                   : "=r"(done) : "r"(smem_addr(&bar)), "r"((uint32_t)(c & 1)) : "memory");
+                   : "=r"(done) : "r"(smem_addr(&bar)), "r"((uint32_t)(tap & 1)) : "memory");
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
-  // epilogue: rows warp*32 + lane of TMEM, 8 columns at a time
-  const int r = warp * 32 + lane;
-  const int oy = y0 + r / TC_TX, ox = x0 + r % TC_TX;
-  const bool inside = oy < H && ox < W;
+  // epilogue: TMEM row i = output position q0 + i
+  const int q = q0 + warp * 32 + lane, oy = q / P - 1, ox = q % P - 1;
+  const bool inside = oy >= 0 && oy < H && ox >= 0 && ox < W;
 #pragma unroll 1
   for (int c0 = 0; c0 < NP; c0 += 8) {
     uint32_t v[8];
@@ -419,13 +424,17 @@ size_t dn_wgrad_scratch_floats(int co, int ci) { return (size_t)kWgChunks * ((si
 template <int NP>
 cudaError_t launch_tc(const float* in, int64_t in_ns, int ci, float* out, int64_t out_ns, int co, int n, int h,
                       int w, const float* weight, const float* bias, bool relu, cudaStream_t s) {
-  const size_t smem = (size_t)(4 * 128 * 2 + 4 * NP * 2) * 16;
-  static bool attr = false;
+  const size_t smem = tc_smem_bytes(ci, w, NP);
+  if (smem > (size_t)TC_MAX_SMEM) return cudaErrorInvalidValue;
+  static bool attr = false;  // per instantiation; the same limit on every device
   if (!attr) {
-    cudaFuncSetAttribute(k_conv3x3_tc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t e = cudaFuncSetAttribute(k_conv3x3_tc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_MAX_SMEM);
+    if (e != cudaSuccess) return e;
     attr = true;
   }
-  const dim3 grid((w + TC_TX - 1) / TC_TX, (h + TC_TY - 1) / TC_TY, n);
+  const int P = w + 2;
+  const int64_t span = (int64_t)(h - 1) * P + w;  // output positions from the first to the last pixel
+  const dim3 grid((unsigned)((span + 127) / 128), n);
   k_conv3x3_tc<NP><<<grid, 128, smem, s>>>(in, in_ns, ci, out, out_ns, co, h, w, weight, bias, relu ? 1 : 0);
   return cudaGetLastError();
 }
