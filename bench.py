@@ -523,9 +523,9 @@ def bench_denoise(args, ws, rank, local, dist):
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None,
                      "note": f"FLOPs = 3 x 2 x sum(ci co 9 H_l W_l) per pixel = {flop_pix:.0f}; forward and "
-                             f"data-gradient convolutions on tcgen05 (bf16 operands, f32 accumulation), weight "
-                             f"gradients in f32 on the CUDA cores; im2col staging from NCHW f32 bounds the "
-                             f"tensor-core kernel; peak = bf16 dense, {pk}"},
+                             f"data-gradient convolutions and the weight gradients on tcgen05 (bf16 operands, f32 "
+                             f"accumulation); staging f32 NCHW tensors into bf16 operands bounds them; peak = bf16 "
+                             f"dense, {pk}"},
         "gpu_launches": launches,
         "clocks": clk,
     }

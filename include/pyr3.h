@@ -278,8 +278,16 @@ int pyr3_dn_conv3x3_wgrad(const float *in, int64_t in_ns, int32_t ci, const floa
                           int64_t dout_ns, int32_t co, int32_t n, int32_t h, int32_t w,
                           float *dweight, float *dbias, float *scratch, uint64_t scratch_floats,
                           void *stream);
-/* Floats of scratch pyr3_dn_conv3x3_wgrad needs for co x ci channels (0 for
- * non-positive sizes). */
+/* pyr3_dn_conv3x3_wgrad on the tensor cores (tcgen05): per tap a GEMM over
+ * pixel positions with input and output gradient rounded to bf16 and f32
+ * accumulation; co, ci <= 128 and n <= 32 (PYR3_E_INVALID otherwise), the
+ * same scratch. */
+int pyr3_dn_conv3x3_wgrad_bf16(const float *in, int64_t in_ns, int32_t ci, const float *dout,
+                               int64_t dout_ns, int32_t co, int32_t n, int32_t h, int32_t w,
+                               float *dweight, float *dbias, float *scratch, uint64_t scratch_floats,
+                               void *stream);
+/* Floats of scratch pyr3_dn_conv3x3_wgrad(_bf16) needs for co x ci channels
+ * (0 for non-positive sizes). */
 uint64_t pyr3_dn_wgrad_scratch_floats(int32_t co, int32_t ci);
 /* flipped[ci][co][k] = weight[co][ci][8-k]: pyr3_dn_conv3x3 with these
  * weights (co and ci swapped, no bias) maps an output gradient to the

@@ -1045,6 +1045,20 @@ PYR3_API int pyr3_dn_conv3x3_wgrad(const float* in, int64_t in_ns, int32_t ci, c
   return PYR3_OK;
 }
 
+PYR3_API int pyr3_dn_conv3x3_wgrad_bf16(const float* in, int64_t in_ns, int32_t ci, const float* dout,
+                                        int64_t dout_ns, int32_t co, int32_t n, int32_t h, int32_t w,
+                                        float* dweight, float* dbias, float* scratch, uint64_t scratch_floats,
+                                        void* stream) {
+  if (!in || !dout || !dweight || !scratch || !dn_dims_ok(ci, co, n, (int64_t)h * w) || h <= 0 || w <= 0 ||
+      co > 128 || ci > 128 || n > 32)
+    return fail(PYR3_E_INVALID, "conv3x3_wgrad_bf16: null operand or size out of range");
+  if (scratch_floats < pyr3::dn_wgrad_scratch_floats(co, ci))
+    return fail(PYR3_E_INVALID, "conv3x3_wgrad_bf16: scratch smaller than pyr3_dn_wgrad_scratch_floats");
+  CUDA_TRY(pyr3::dn_conv3x3_wgrad_bf16(in, in_ns, ci, dout, dout_ns, co, n, h, w, dweight, dbias, scratch,
+                                       (cudaStream_t)stream));
+  return PYR3_OK;
+}
+
 PYR3_API uint64_t pyr3_dn_wgrad_scratch_floats(int32_t co, int32_t ci) {
   return co > 0 && ci > 0 ? (uint64_t)pyr3::dn_wgrad_scratch_floats(co, ci) : 0;
 }

@@ -140,11 +140,11 @@ k_wgrad_part(const float* __restrict__ in, int64_t in_ns, int ci_n, const float*
   }
 }
 
-__global__ void k_wgrad_reduce(const float* __restrict__ part, int64_t per, float* __restrict__ out) {
+__global__ void k_wgrad_reduce(const float* __restrict__ part, int64_t per, int parts, float* __restrict__ out) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= per) return;
   float x = 0.0f;
-  for (int s = 0; s < kWgChunks; ++s) x += part[s * per + i];
+  for (int s = 0; s < parts; ++s) x += part[s * per + i];
   out[i] = x;
 }
 
@@ -410,6 +410,145 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL) : "memory");
 }
 
+// ---- weight gradient on the tensor cores
+// dW[co][ci][tap] = sum over positions q of dout[q][co] * in[q + d_tap][ci],
+// q over the zero-padded grid (P = W + 2), so for each tap it is a GEMM
+// with M = output channels (padded to 128), N = input channels (padded to
+// NP), K = positions.  CTA (chunk c, image n, tap) reduces its chunk of
+// positions in steps of 64: the 128 threads stage dout rows (A, zero at
+// padding positions) and the tap-shifted input rows (B) as bf16 in the
+// canonical K-major layout, one thread issues four K = 16 MMAs into TMEM
+// and commits to the mbarrier (bounded waits); the epilogue writes the
+// chunk's partial dW[co][ci][tap] to part[c * n_img + n], which
+// k_wgrad_reduce adds in a fixed order.
+constexpr int WT_KC = 64;
+
+template <int NP>
+__global__ void __launch_bounds__(128)
+k_wgrad_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, const float* __restrict__ dout,
+           int64_t dout_ns, int co_n, int H, int W, int chunk, float* __restrict__ part) {
+  constexpr uint32_t NCOL = NP <= 32 ? 32 : (NP <= 64 ? 64 : 128);
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint4* sa = reinterpret_cast<uint4*>(smem);  // 4 K steps x 128 rows x 2 halves x 16 B
+  uint4* sb = sa + 4 * 128 * 2;                 // 4 K steps x NP rows x 2 halves x 16 B
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int c = blockIdx.x, n = blockIdx.y, tap = blockIdx.z;
+  const int P = W + 2;
+  const int d = (tap / 3 - 1) * P + (tap % 3 - 1);
+  const int q_begin = P + 1 + c * chunk;
+  const int q_end = min(q_begin + chunk, H * P + W + 1);  // past the last interior position
+  const int64_t hw = (int64_t)H * W;
+  const float* dn = dout + n * dout_ns;
+  const float* ip = in + n * in_ns;
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n"
+                 "fence.mbarrier_init.release.cluster;" ::"r"(smem_addr(&bar)) : "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base)),
+                 "r"(NCOL) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NP >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  int phase = 0;
+  for (int qs = q_begin; qs < q_end; qs += WT_KC, ++phase) {
+    // A rows: output channel co (128 rows), 8 positions per 16-byte row
+    for (int idx = t; idx < 128 * (WT_KC / 8); idx += 128) {
+      const int co = idx >> 3, g = idx & 7;
+      float v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int q = qs + g * 8 + j, y = q / P - 1, x = q % P - 1;
+        v[j] = (co < co_n && q < q_end && y >= 0 && y < H && x >= 0 && x < W) ? dn[co * hw + (int64_t)y * W + x]
+                                                                             : 0.0f;
+      }
+      const int s = g >> 1, h = g & 1;
+      sa[(s * 32 + (co >> 3) * 2 + h) * 8 + (co & 7)] =
+          make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
+    }
+    // B rows: input channel ci, the positions shifted by the tap
+    for (int idx = t; idx < NP * (WT_KC / 8); idx += 128) {
+      const int ci = idx >> 3, g = idx & 7;
+      float v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int q = qs + g * 8 + j, qi = q + d, y = qi / P - 1, x = qi % P - 1;
+        v[j] = (ci < ci_n && q < q_end && y >= 0 && y < H && x >= 0 && x < W) ? ip[ci * hw + (int64_t)y * W + x]
+                                                                             : 0.0f;
+      }
+      const int s = g >> 1, h = g & 1;
+      sb[(s * (NP / 4) + (ci >> 3) * 2 + h) * 8 + (ci & 7)] =
+          make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int s = 0; s < 4; ++s) {
+        const uint64_t da = umma_desc(smem_addr(sa + (size_t)s * 128 * 2), 128u, 256u);
+        const uint64_t db = umma_desc(smem_addr(sb + (size_t)s * NP * 2), 128u, 256u);
+        const uint32_t acc = (phase > 0 || s > 0) ? 1u : 0u;
+        asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                     ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   ::"r"(smem_addr(&bar)) : "memory");
+    }
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < TC_WAIT_LIMIT && !done; ++it)
+      asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                   : "=r"(done) : "r"(smem_addr(&bar)), "r"((uint32_t)(phase & 1)) : "memory");
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  // epilogue: TMEM row co, column ci (a chunk without positions leaves zeros)
+  const int co = warp * 32 + lane;
+  float* pp = part + (int64_t)(c * gridDim.y + n) * co_n * ci_n * 9;
+#pragma unroll 1
+  for (int c0 = 0; c0 < NP; c0 += 8) {
+    uint32_t v[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (co < co_n) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int ci = c0 + j;
+        if (ci < ci_n) pp[((int64_t)co * ci_n + ci) * 9 + tap] = phase > 0 ? __uint_as_float(v[j]) : 0.0f;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL) : "memory");
+}
+
+__global__ void __launch_bounds__(256)
+k_bias_part(const float* __restrict__ dout, int64_t dout_ns, int co_n, int n_img, int64_t hw, float* part_b) {
+  // block (co, chunk s): sum of dout[co] over chunk s of all images' pixels
+  const int co = blockIdx.x, s = blockIdx.y;
+  const int64_t P = hw * n_img, p0 = P * s / kWgChunks, p1 = P * (s + 1) / kWgChunks;
+  float a = 0.0f;
+  for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) a += dout[(p / hw) * dout_ns + co * hw + p % hw];
+  __shared__ float red[8];
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float v = 0.0f;
+    for (int j = 0; j < (int)(blockDim.x >> 5); ++j) v += red[j];
+    part_b[(int64_t)s * co_n + co] = v;
+  }
+}
+
 }  // namespace
 
 cudaError_t dn_conv3x3(const float* in, int64_t in_ns, int ci, float* out, int64_t out_ns, int co, int n,
@@ -420,6 +559,48 @@ cudaError_t dn_conv3x3(const float* in, int64_t in_ns, int ci, float* out, int64
 }
 
 size_t dn_wgrad_scratch_floats(int co, int ci) { return (size_t)kWgChunks * ((size_t)co * ci * 9 + co); }
+
+template <int NP>
+cudaError_t launch_wgrad_tc(const float* in, int64_t in_ns, int ci, const float* dout, int64_t dout_ns, int co,
+                            int n, int h, int w, float* part, cudaStream_t s) {
+  const size_t smem = (size_t)(4 * 128 * 2 + 4 * NP * 2) * 16;
+  static bool attr = false;  // per instantiation; the same limit on every device
+  if (!attr) {
+    const cudaError_t e = cudaFuncSetAttribute(k_wgrad_tc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  // kWgChunks partials in all: chunks per image x images
+  const int per_img = std::max(1, kWgChunks / n);
+  const int64_t span = (int64_t)(h - 1) * (w + 2) + w;
+  const int chunk = (int)(((span + per_img - 1) / per_img + WT_KC - 1) / WT_KC * WT_KC);
+  k_wgrad_tc<NP><<<dim3(per_img, n, 9), 128, smem, s>>>(in, in_ns, ci, dout, dout_ns, co, h, w, chunk, part);
+  return cudaGetLastError();
+}
+
+cudaError_t dn_conv3x3_wgrad_bf16(const float* in, int64_t in_ns, int ci, const float* dout, int64_t dout_ns,
+                                  int co, int n, int h, int w, float* dw, float* db, float* scratch, cudaStream_t s) {
+  if (co > 128 || n > kWgChunks) return cudaErrorInvalidValue;
+  const int per_img = std::max(1, kWgChunks / n), parts = per_img * n;
+  const int64_t per_w = (int64_t)co * ci * 9;
+  float* part = scratch;
+  float* part_b = scratch + (int64_t)kWgChunks * per_w;
+  cudaError_t e;
+  if (ci <= 16) e = launch_wgrad_tc<16>(in, in_ns, ci, dout, dout_ns, co, n, h, w, part, s);
+  else if (ci <= 32) e = launch_wgrad_tc<32>(in, in_ns, ci, dout, dout_ns, co, n, h, w, part, s);
+  else if (ci <= 48) e = launch_wgrad_tc<48>(in, in_ns, ci, dout, dout_ns, co, n, h, w, part, s);
+  else if (ci <= 64) e = launch_wgrad_tc<64>(in, in_ns, ci, dout, dout_ns, co, n, h, w, part, s);
+  else if (ci <= 96) e = launch_wgrad_tc<96>(in, in_ns, ci, dout, dout_ns, co, n, h, w, part, s);
+  else if (ci <= 128) e = launch_wgrad_tc<128>(in, in_ns, ci, dout, dout_ns, co, n, h, w, part, s);
+  else return cudaErrorInvalidValue;
+  if (e != cudaSuccess) return e;
+  k_wgrad_reduce<<<blocks_for(per_w), 256, 0, s>>>(part, per_w, parts, dw);
+  if (db) {
+    k_bias_part<<<dim3(co, kWgChunks), 256, 0, s>>>(dout, dout_ns, co, n, (int64_t)h * w, part_b);
+    k_wgrad_reduce<<<blocks_for(co), 256, 0, s>>>(part_b, co, kWgChunks, db);
+  }
+  return cudaGetLastError();
+}
 
 template <int NP>
 cudaError_t launch_tc(const float* in, int64_t in_ns, int ci, float* out, int64_t out_ns, int co, int n, int h,
@@ -458,8 +639,8 @@ cudaError_t dn_conv3x3_wgrad(const float* in, int64_t in_ns, int ci, const float
   float* part_b = scratch + kWgChunks * per_w;
   const dim3 grid((ci + WG_CI - 1) / WG_CI, (co + WG_CO - 1) / WG_CO, kWgChunks);
   k_wgrad_part<<<grid, 256, 0, s>>>(in, in_ns, ci, dout, dout_ns, co, n, h, w, part, part_b);
-  k_wgrad_reduce<<<blocks_for(per_w), 256, 0, s>>>(part, per_w, dw);
-  if (db) k_wgrad_reduce<<<blocks_for(co), 256, 0, s>>>(part_b, co, db);
+  k_wgrad_reduce<<<blocks_for(per_w), 256, 0, s>>>(part, per_w, kWgChunks, dw);
+  if (db) k_wgrad_reduce<<<blocks_for(co), 256, 0, s>>>(part_b, co, kWgChunks, db);
   return cudaGetLastError();
 }
 

@@ -26,6 +26,12 @@ size_t dn_wgrad_scratch_floats(int co, int ci);
 cudaError_t dn_conv3x3_wgrad(const float* in, int64_t in_ns, int ci, const float* dout,
                              int64_t dout_ns, int co, int n, int h, int w, float* dw, float* db,
                              float* scratch, cudaStream_t s);
+// The same gradients on the tensor cores (tcgen05): per tap a GEMM over the
+// padded grid's positions with bf16 operands and f32 accumulation; co <= 128,
+// ci <= 128, n <= 32; the same scratch.
+cudaError_t dn_conv3x3_wgrad_bf16(const float* in, int64_t in_ns, int ci, const float* dout,
+                                  int64_t dout_ns, int co, int n, int h, int w, float* dw, float* db,
+                                  float* scratch, cudaStream_t s);
 // wt[ci][co][k] = w[co][ci][8 - k]: the data gradient of a 3x3 convolution
 // is the convolution of dout with these weights.
 cudaError_t dn_flip_weights(const float* w, int co, int ci, float* wt, cudaStream_t s);

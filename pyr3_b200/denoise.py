@@ -1,7 +1,7 @@
 """Learned denoiser: a small U-Net that maps a low-sample render (8 feature
 channels) to the colours of a high-sample render of the same genome,
 trained and run with this library's CUDA layers (pyr3_dn_* in the C-ABI):
-the forward and data-gradient convolutions on the tensor cores (tcgen05,
+the convolutions and their weight gradients on the tensor cores (tcgen05,
 bf16 operands, f32 accumulation) by default, or all in f32.
 The denoiser has no counterpart in the reference.
 
@@ -180,8 +180,9 @@ class UNet:
         self.launches += 3
         dw, db = self._gw(i)
         h, wd = self.hs[l]
-        _check(_lib.lib().pyr3_dn_conv3x3_wgrad(src[0], src[1], ci, g[0], g[1], co, self.n, h, wd, dw, db,
-                                                C.c_void_p(self.wsc.data_ptr()), self.wsc_n, self._stream()))
+        fn = _lib.lib().pyr3_dn_conv3x3_wgrad_bf16 if self.tc else _lib.lib().pyr3_dn_conv3x3_wgrad
+        _check(fn(src[0], src[1], ci, g[0], g[1], co, self.n, h, wd, dw, db, C.c_void_p(self.wsc.data_ptr()),
+                  self.wsc_n, self._stream()))
 
     def _mask(self, g, y, c, l):
         self.launches += 1

@@ -156,6 +156,21 @@ def test_cuda_layers_match_oracle():
                          None, 0, None))
     torch.cuda.synchronize()
     _close(dx, D.conv3x3_dgrad(g, wt))
+    # tensor-core weight gradient: the oracle on bf16-rounded operands, f32 sums
+    for co2, ci2 in ((co, ci), (90, 40)):
+        x2, g2 = rng.normal(size=(n, ci2, h, w)), rng.normal(size=(n, co2, h, w))
+        x2d, g2d = _dev(x2), _dev(g2)
+        dw2 = torch.zeros((co2, ci2, 3, 3), device="cuda")
+        db2 = torch.zeros(co2, device="cuda")
+        nsc2 = L.pyr3_dn_wgrad_scratch_floats(co2, ci2)
+        sc2 = torch.zeros(nsc2, device="cuda")
+        ck(L.pyr3_dn_conv3x3_wgrad_bf16(_p(x2d), ci2 * h * w, ci2, _p(g2d), co2 * h * w, co2, n, h, w,
+                                        C.c_void_p(dw2.data_ptr()), C.c_void_p(db2.data_ptr()),
+                                        C.c_void_p(sc2.data_ptr()), nsc2, None))
+        torch.cuda.synchronize()
+        rdw, rdb = D.conv3x3_wgrad(_bf16(x2), _bf16(g2))
+        _close(dw2, rdw, rtol=1e-4, atol=1e-3)
+        _close(db2, D.conv3x3_wgrad(x2, g2.astype(np.float32).astype(np.float64))[1], rtol=1e-4, atol=1e-3)
     # tensor-core convolution: the oracle on bf16-rounded operands, f32 sums
     for co2 in (co, 40, 90):
         w2 = rng.normal(size=(co2, ci, 3, 3)) * 0.2
