@@ -472,7 +472,22 @@ def bench_denoise(args, ws, rank, local, dist):
     launches = net.launches
     clk = clocks.stop() if clocks else None
     t_max = _max_over_ranks(ms, dist, local)
-    p_noisy, p_dn, _ = DN.evaluate(net.params(), xho, tho)
+    p_noisy, p_dn, dn_img = DN.evaluate(net.params(), xho, tho)
+    ssim_in = DN.ssim(np.clip(xho[:, :3], 0.0, 1.0), tho)
+    ssim_dn = DN.ssim(dn_img, tho)
+    # time to quality: plain renders of the held-out genomes at rising spp against the
+    # same 2000-spp targets, and the denoiser's inference time for all of them
+    plain = DN.plain_quality(gs[64:], tho, (25, 50, 100, 200, 400, 800))
+    inet = DN.UNet(len(xho), 256, 256, net.params())
+    inet.set_batch(xho)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    inet.forward()
+    e0.record()
+    inet.forward()
+    e1.record()
+    e1.synchronize()
+    infer_ms = e0.elapsed_time(e1)
+    match = next((p for p in plain if p[1] >= p_dn), None)
     # e2e: batches assembled on the host, uploaded each step, loss read back each step
     rng = np.random.default_rng(3)
     hnet = DN.UNet(batch, crop, crop, net.params())
@@ -516,6 +531,11 @@ def bench_denoise(args, ws, rank, local, dist):
                    "adam_steps_per_step": per, "l2": "inputs resident; working set < L2 per layer",
                    "parallelism": f"replicas x{ws}"},
         "quality": {"held_out_psnr_input_db": p_noisy, "held_out_psnr_denoised_db": p_dn,
+                    "held_out_ssim_input": ssim_in, "held_out_ssim_denoised": ssim_dn,
+                    "plain_render_psnr_by_spp": [[p[0], round(p[1], 3), round(p[2], 3)] for p in plain],
+                    "plain_spp_matching_denoised": match[0] if match else None,
+                    "time_to_denoised_quality_ms": {"denoised": round(plain[0][2] + infer_ms, 3),
+                                                    "plain": round(match[2], 3) if match else None},
                     "train_loss_first_last": [losses[0][1], losses[-1][1]],
                     "adam_steps_total": per * (args.warmup + args.steps), "render_seconds": render_s},
         "e2e": {"value": ws * pix_step * n_e2e / (e2e_max / 1e3), "unit": "pixels/s",

@@ -349,6 +349,23 @@ def target(renderer, genome, samples: int) -> np.ndarray:
     return np.ascontiguousarray(img[..., :3].transpose(2, 0, 1))
 
 
+def ssim(a: np.ndarray, b: np.ndarray) -> float:
+    """Mean SSIM (Wang et al. 2004: 11x11 Gaussian window, sigma 1.5,
+    K1 = 0.01, K2 = 0.03, dynamic range 1) over images and channels of
+    N x C x H x W arrays in 0..1."""
+    from scipy.ndimage import gaussian_filter
+
+    c1, c2 = 0.01 ** 2, 0.03 ** 2
+    vals = []
+    for x, y in zip(a.reshape(-1, *a.shape[-2:]).astype(np.float64), b.reshape(-1, *b.shape[-2:]).astype(np.float64)):
+        f = lambda z: gaussian_filter(z, 1.5, truncate=3.5)  # noqa: E731  (11-tap window)
+        mx, my = f(x), f(y)
+        sxx, syy, sxy = f(x * x) - mx * mx, f(y * y) - my * my, f(x * y) - mx * my
+        vals.append(float((((2 * mx * my + c1) * (2 * sxy + c2)) /
+                           ((mx * mx + my * my + c1) * (sxx + syy + c2))).mean()))
+    return float(np.mean(vals))
+
+
 def psnr(a: np.ndarray, b: np.ndarray) -> float:
     mse = float(((a.astype(np.float64) - b) ** 2).mean())
     return 10.0 * np.log10(1.0 / max(mse, 1e-20))
@@ -413,3 +430,24 @@ def evaluate(params, xs, ts, chans=CHANS, tensor_cores: bool = True):
     net.forward()
     out = np.clip(net.output(), 0.0, 1.0)
     return psnr(np.clip(xs[:, :3], 0.0, 1.0), ts), psnr(out, ts), out
+
+
+def plain_quality(genomes, targets, spps, seed: int = 99):
+    """PSNR against `targets` of plain renders of `genomes` at each spp in
+    `spps`, with the device time of those renders: [(spp, psnr, ms)]."""
+    from . import renderer as R
+
+    W, H = genomes[0].size
+    r = R.create_renderer(W, H, 1)
+    res = []
+    for spp in spps:
+        imgs, ms = [], 0.0
+        for i, g in enumerate(genomes):
+            w, it, samples = R.compute_dispatch(spp, W, H)
+            r.reset(g)
+            r.iterate(g, seed + i, w, it)
+            ms += r.last_iterate_ms()
+            imgs.append(target(r, g, samples))
+        res.append((spp, psnr(np.stack(imgs), targets), ms))
+    r.destroy()
+    return res
