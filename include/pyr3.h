@@ -155,10 +155,11 @@ int pyr3_read_histogram(pyr3_renderer *r, uint32_t *host_out);
  * scene-referred values (k1, k2 from deriveCalibration, src/calibration.ts). */
 int pyr3_read_linear(pyr3_renderer *r, double k1, double k2, float *host_out);
 /* ---- batches ---------------------------------------------------------- */
-/* Batched rendering of many genomes in one CUDA graph (the north_star's
- * batched persistent launch; no counterpart in the reference, which renders
- * genomes one dispatch at a time).  renderers[i] renders genomes[i] with
- * opts[i] (walkers x iters_per_walker samples; without
+/* Batched rendering of many genomes (no counterpart in the reference,
+ * which renders genomes one dispatch at a time): genomes too small to fill
+ * the GPU share one CUDA graph, genomes of 2^24 samples or more run beside
+ * it through pyr3_iterate, one after another.  renderers[i] renders
+ * genomes[i] with opts[i] (walkers x iters_per_walker samples; without
  * PYR3_ITER_EXACT_WALKERS the batch picks its own walker count per genome).
  * All renderers must be on one device.  pyr3_batch_run clears every
  * renderer's histogram and accumulates its samples, asynchronously, on the
