@@ -28,7 +28,7 @@ extern "C" {
 #define PYR3_E_CUDA (-2)      /* CUDA runtime or driver error */
 #define PYR3_E_NVRTC (-3)     /* JIT compile of the chaos kernel failed */
 #define PYR3_E_NOMEM (-4)     /* device allocation failed */
-#define PYR3_E_UNSUPPORTED (-5) /* variation index not in this build */
+#define PYR3_E_UNSUPPORTED (-5) /* variation index not implemented by this library */
 
 #define PYR3_XFORM_FLOATS 116  /* packed xform record (src/genome.ts:293-313) */
 #define PYR3_MAX_XFORMS 128    /* src/genome.ts:326 */
@@ -330,7 +330,7 @@ int pyr3_jit_compile_variation(uint32_t idx, uint64_t *cubin_bytes);
  * no-prior row) as the renderer reproduces it from its per-row boundaries. */
 int pyr3_pick_table(uint32_t n_xforms, const float *weights, const float *xaos,
                     uint32_t *table_out);
-/* 1 if this build implements variation idx, 0 if not; name via *name. */
+/* 1 if this library implements variation idx, 0 if not; name via *name. */
 int pyr3_variation_info(uint32_t idx, int32_t *implemented, int32_t *is_dc, const char **name);
 
 #ifdef __cplusplus

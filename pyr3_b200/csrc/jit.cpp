@@ -254,7 +254,7 @@ static std::string shape_one(const float* X, XformShape* s) {
       s->vars.push_back(-1);  // the reference's default case contributes (0, 0)
     } else {
       return std::string("variation ") + std::to_string(idx) + " (" + variation_name(idx) +
-             ") is not implemented in this build";
+             ") is not implemented in this library";
     }
   }
   // Out-of-range indices contribute nothing: drop them from the generated code.

@@ -102,7 +102,7 @@ std::string chaos_source(const GenomeShape& s, int wpb, bool aggregate);
 int compile_eval_only(int idx, size_t* bytes, std::string* err);
 // Module with the variation evaluator for variation `idx`.
 int get_eval_module(int idx, std::shared_ptr<EvalModule>* out, std::string* err);
-// True if this build's variation library implements `idx`.
+// True if the variation library implements `idx`.
 bool variation_implemented(int idx);
 const char* variation_name(int idx);
 bool variation_is_dc(int idx);
