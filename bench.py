@@ -253,6 +253,16 @@ def bench_ours(args, ws, rank, local, dist):
     _barrier(dist)
     t_max = _max_over_ranks(total_ms, dist, local)
 
+    # Scatter roofline: the same number of 4-atomic splats into uniformly
+    # random cells of this histogram (pyr3_splat_rate), against the chaos
+    # kernel's splats per second.  The histogram is reset by every step below.
+    srate = None
+    if n_splats > 0:
+        sms = C.c_float()
+        _lib.check(lib.pyr3_splat_rate(h, n_splats, C.byref(sms)))
+        _lib.check(lib.pyr3_splat_rate(h, n_splats, C.byref(sms)))
+        srate = n_splats / (sms.value / 1e3)
+
     # e2e through the public API: host palette + genome in, RGBA8 image out
     host_img = np.zeros((H, W, 4), np.uint8)
     def step_public(seed):
@@ -320,6 +330,11 @@ def bench_ours(args, ws, rank, local, dist):
                              f"32 B (16 B bucket read+write) per in-canvas splat ({splats_per_launch:.0f} "
                              f"splats per launch); peak {peak_kind}; the kernel is bound by instruction "
                              f"issue and latency (ncu), not by HBM"},
+        "scatter_roofline": None if srate is None else {
+            "achieved": n_splats / (mean_chaos / 1e3), "peak": srate, "unit": "splats/s",
+            "frac": n_splats / (mean_chaos / 1e3) / srate,
+            "note": "a splat = 4 saturating u32 atomics on one 16-byte bucket; peak = the same splats "
+                    "into uniformly random buckets of this histogram (pyr3_splat_rate), measured here"},
         "gpu_launches": chaos_launches + args.steps * (1 + (1 if g.density is not None else 0)),
         "clocks": clk,
     }

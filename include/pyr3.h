@@ -195,6 +195,11 @@ int pyr3_last_iterate_launches(pyr3_renderer *r, uint64_t *launches);
  * then read the device time between two marks (waits for the later one). */
 int pyr3_mark(pyr3_renderer *r, int32_t slot);
 int pyr3_elapsed(pyr3_renderer *r, int32_t a, int32_t b, float *ms);
+/* Measurement: device time (*ms) of `splats` deposits of 4 saturating u32
+ * atomics, the chaos kernel's scatter, into uniformly random cells of the
+ * renderer's histogram -- the random-scatter rate its splats are measured
+ * against.  Leaves the histogram's contents changed (call pyr3_reset). */
+int pyr3_splat_rate(pyr3_renderer *r, uint64_t splats, float *ms);
 /* Overwrite a scratch buffer of `bytes` on the renderer's stream (evicts
  * the L2 between timed steps). */
 int pyr3_flush_l2(pyr3_renderer *r, uint64_t bytes);

@@ -97,6 +97,7 @@ _SIGS = {
                                         C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_uint64, C.c_void_p]),
     "pyr3_dn_wgrad_scratch_floats": (C.c_uint64, [C.c_int32, C.c_int32]),
+    "pyr3_splat_rate": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_float)]),
     "pyr3_dn_conv3x3_wgrad_bf16": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_int64, C.c_int32,
                                              C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_uint64, C.c_void_p]),

@@ -1620,6 +1620,17 @@ PYR3_API int pyr3_elapsed(pyr3_renderer* r, int32_t a, int32_t b, float* ms) {
   return PYR3_OK;
 }
 
+PYR3_API int pyr3_splat_rate(pyr3_renderer* r, uint64_t splats, float* ms) {
+  if (!r || !ms || splats == 0) return fail(PYR3_E_INVALID, "bad arguments");
+  cudaSetDevice(r->device);
+  CUDA_TRY(cudaEventRecord(r->ev0, r->stream));
+  CUDA_TRY(pyr3::launch_splat_rate(r->d_hist, (uint64_t)r->SW * r->SH, splats, device_sms(r->device), r->stream));
+  CUDA_TRY(cudaEventRecord(r->ev1, r->stream));
+  CUDA_TRY(cudaEventSynchronize(r->ev1));
+  CUDA_TRY(cudaEventElapsedTime(ms, r->ev0, r->ev1));
+  return PYR3_OK;
+}
+
 PYR3_API int pyr3_flush_l2(pyr3_renderer* r, uint64_t bytes) {
   if (!r) return fail(PYR3_E_INVALID, "null renderer");
   cudaSetDevice(r->device);

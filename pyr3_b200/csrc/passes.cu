@@ -377,4 +377,30 @@ cudaError_t launch_linear_export(const uint32_t* hist, uint32_t width, uint32_t 
   return cudaGetLastError();
 }
 
+
+namespace {
+// Each thread walks an LCG over cells and deposits 1 into the 4 channels of
+// each, with the chaos kernel's saturation check on the returned values.
+__global__ void __launch_bounds__(256) k_splat_rate(uint32_t* cells, uint64_t n_cells, uint64_t per_thread,
+                                                    uint64_t extra) {
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t n = per_thread + (tid < extra ? 1 : 0);
+  uint32_t x = (uint32_t)(tid * 2654435761ull) ^ 0x9e3779b9u;
+  for (uint64_t i = 0; i < n; ++i) {
+    x = x * 1664525u + 1013904223u;
+    uint32_t* c = cells + ((uint64_t)x * n_cells >> 32) * 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t old = atomicAdd(c + k, 1u);
+      if (old > 0xffffffffu - 1u) atomicOr(c + k, 0xffffffffu);
+    }
+  }
+}
+}  // namespace
+
+cudaError_t launch_splat_rate(uint32_t* cells, uint64_t n_cells, uint64_t splats, int sms, cudaStream_t s) {
+  const uint64_t threads = (uint64_t)sms * 8 * 256;
+  k_splat_rate<<<(unsigned)(sms * 8), 256, 0, s>>>(cells, n_cells, splats / threads, splats % threads);
+  return cudaGetLastError();
+}
 }  // namespace pyr3

@@ -38,6 +38,9 @@ cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, cons
 // histogramToLinearRgba (src/export-linear.ts:24-47): box-collapse of each
 // oversample x oversample block in f64, scaled by k1 * k2 / oversample^2;
 // coverage (alpha) clamped to [0, 1].  out = width x height x RGBA f32.
+// Random-splat atomic rate: `splats` deposits of 4 saturating u32 atomics
+// (the chaos kernel's scatter) into uniformly random cells of `cells`.
+cudaError_t launch_splat_rate(uint32_t* cells, uint64_t n_cells, uint64_t splats, int sms, cudaStream_t s);
 cudaError_t launch_linear_export(const uint32_t* hist, uint32_t width, uint32_t height,
                                  uint32_t oversample, double k1, double k2, float* out,
                                  cudaStream_t s);
