@@ -466,3 +466,16 @@ def test_kernel_autotuner_splits_the_first_large_launch():
     hist, _, _ = r.read_histogram()
     assert int(hist.reshape(-1, 4)[:, 3].astype(np.uint64).sum()) == 255 * n_in
     r.destroy()
+
+
+def test_splat_rate_deposits_every_splat():
+    """pyr3_splat_rate (the scatter roofline's measurement) lands every one of
+    its splats: each channel of the histogram sums to the splat count."""
+    r = R.create_renderer(320, 240, 1)
+    r.reset(workloads.plain_small())
+    ms = C.c_float()
+    _lib.check(_lib.lib().pyr3_splat_rate(r.handle, 1_000_003, C.byref(ms)))
+    hist, _, _ = r.read_histogram()
+    sums = hist.reshape(-1, 4).astype(np.uint64).sum(axis=0)
+    assert ms.value > 0.0 and [int(v) for v in sums] == [1_000_003] * 4
+    r.destroy()
