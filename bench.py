@@ -37,6 +37,7 @@ CONFIGS = {
     "motion_4k": ("iters/s (4K, 6 xforms, 8 temporal samples)", "motion_4k"),
     "batch_256": ("iters/s (256 genomes, batched)", "batch_256"),
     "denoise": ("denoiser training pixels/s (U-Net fwd+bwd+Adam)", "denoise_set"),
+    "exposure": ("auto-exposure passes/s (1080p os 2 present + 1024-edge probe)", "headline_1080p"),
 }
 
 
@@ -566,6 +567,121 @@ def bench_denoise(args, ws, rank, local, dist):
     }
 
 
+def bench_exposure(args, ws, rank, local, dist):
+    """Render-time auto-exposure (bin/pyr3-render.ts:487-513) after the
+    headline render: a step = the preview probe (1024 x 576, 16 spp, fixed
+    seed: chaos, present, device mean luminance) and the brightness fit on
+    the 1920x1080 os-2 histogram (present, device mean, up to 4
+    re-presents; 8 bytes read back per pass).  The loop is host-driven, so
+    a step is timed on the host clock between device synchronisations."""
+    import time as _t
+
+    import torch
+
+    from oracle import auto_exposure as OA
+    from oracle import oracle as O
+    from pyr3_b200 import _lib, auto_exposure as AE, renderer as R
+
+    g, _ = _workload("headline")
+    W, H = g.size
+    r = R.create_renderer(W, H, g.oversample, g.filter_radius, device=local)
+    walkers, iters, samples = R.compute_dispatch(g.quality, W, H)
+    if args.samples:  # profiling case: a smaller high-quality histogram (untimed)
+        walkers, iters = 1024, max(1, args.samples // 1024)
+        samples = walkers * iters
+    r.reset(g)
+    r.iterate(g, 1, walkers, iters)
+    probe_r = R.create_renderer(16, 16, 1, device=local)
+    img = torch.empty((H, W, 4), dtype=torch.uint8, device=f"cuda:{local}")
+    host = torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True)
+    lib = _lib.lib()
+
+    def step(e2e=False):
+        target = AE.measure_probe_luminance(g, renderer=probe_r)
+        fit, _ = AE.auto_expose(r, g, samples, target, image=img)
+        if e2e:
+            host.copy_(img)
+        return target, fit
+
+    per = 20  # passes per bench step, so the clock sampler sees the timed region
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    _barrier(dist)
+    clocks = Clocks(local) if rank == 0 else None
+    l0 = r.launches + probe_r.launches
+    t0 = _t.perf_counter()
+    for _ in range(args.steps * per):
+        target, fit = step()
+    torch.cuda.synchronize()
+    step_s = (_t.perf_counter() - t0) / (args.steps * per)
+    chaos_launches = (r.launches + probe_r.launches - l0) / (args.steps * per)
+    clk = clocks.stop() if clocks else None
+    t0 = _t.perf_counter()
+    for _ in range(args.steps * per):
+        step(e2e=True)
+    torch.cuda.synchronize()
+    e2e_s = (_t.perf_counter() - t0) / (args.steps * per)
+    # the luminance pass alone: device time of pyr3_mean_luminance on the
+    # 1080p image (memset, kernel, 8-byte read-back)
+    out = C.c_double()
+    reps = 50
+    _lib.check(lib.pyr3_mark(r.handle, 2))
+    for _ in range(reps):
+        _lib.check(lib.pyr3_mean_luminance(r.handle, C.c_void_p(img.data_ptr()), W * H, _lib.OUT_RGBA8,
+                                           C.byref(out)))
+    _lib.check(lib.pyr3_mark(r.handle, 3))
+    lms = C.c_float()
+    _lib.check(lib.pyr3_elapsed(r.handle, 2, 3, C.byref(lms)))
+    luma_ms = lms.value / reps
+    t_max = _max_over_ranks(step_s * 1e3, dist, local)
+    e2e_max = _max_over_ranks(e2e_s * 1e3, dist, local)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        # one re-present pass the reference's way: its visualize shader on
+        # the host cores over the super-res histogram, then the host mean
+        hist, _, _ = r.read_histogram()
+        p = r.present_opts(g)
+        k1, k2 = O.derive_calibration(g.scale, samples, p.brightness, g.oversample)
+        threads = os.cpu_count() or 1
+        t0 = _t.perf_counter()
+        ref = O.ref_visualize(W, H, g.oversample, O.spatial_kernel(0.5, g.oversample), np.float32(k1),
+                              np.float32(k2), p.gamma, p.vibrancy, p.highpow, p.linrange,
+                              bg=tuple(p.background), src_u32=hist.reshape(-1), threads=threads)
+        OA.mean_luminance(np.clip(np.rint(ref * 255.0), 0, 255).astype(np.uint8))
+        cpu_s = _t.perf_counter() - t0
+        cpu = {"value": 1.0 / cpu_s, "unit": "re-present passes/s", "cores": threads, "kind": "reference",
+               "sample": "one 1920x1080 os-2 visualize (the reference's shader on the CPU) + host mean "
+                         "luminance; a full auto-exposure pass adds the probe render and 1-4 more presents"}
+    if rank != 0:
+        return None
+    peak, pk = _peaks()
+    luma_gbs = W * H * 4 / (luma_ms * 1e-3) / 1e9
+    return {
+        "metric": CONFIGS["exposure"][0], "value": ws * 1e3 / t_max, "unit": "passes/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max * per,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (headline genome, pyr3_b200/workloads.py:headline_1080p)",
+        "config": {"workload": "exposure", "canvas": [W, H], "oversample": g.oversample,
+                   "hq_samples": samples, "probe": [1024, 576], "probe_spp": 16,
+                   "passes_per_step": per, "ms_per_pass": t_max,
+                   "probe_target_mean": target, "fit": vars(fit),
+                   "timing": "host clock between synchronisations (host-driven loop)",
+                   "l2": "histogram 133 MB > L2", "parallelism": f"replicas x{ws}"},
+        "e2e": {"value": ws * 1e3 / e2e_max, "unit": "passes/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(W * H * 4 + 8 * (2 + fit.iters)) * per},
+        "roofline": {"bound": "hbm", "achieved": luma_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": luma_gbs / peak, "traffic": None,
+                     "note": f"luminance pass: {W * H * 4} B image read per call / device time of "
+                             f"pyr3_mean_luminance ({luma_ms * 1e3:.1f} us incl. memset and 8-byte read-back); "
+                             f"the pass's dominant kernel is the probe's chaos kernel (9.4e6 samples, 200 "
+                             f"burn-in iterations per walker), reported by the headline config; peak {pk}"},
+        "cpu_baseline": cpu,
+        "gpu_launches": int((chaos_launches + 2 * (1 + fit.iters) + 2) * per),
+        "clocks": clk,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -585,12 +701,18 @@ def main():
         if args.impl == "reference" and args.config == "denoise":
             line = {"impl": "reference", "unavailable": "the reference has no learned denoiser"} \
                 if rank == 0 else None
+        elif args.impl == "reference" and args.config == "exposure":
+            line = {"impl": "reference", "unavailable": "the reference presents only through WebGPU "
+                    "(unavailable on this box); its visualize shader on the CPU is the cpu_baseline"} \
+                if rank == 0 else None
         elif args.impl == "reference":
             line = bench_reference(args, ws, rank, local, dist)
         elif args.config == "batch_256":
             line = bench_batch(args, ws, rank, local, dist)
         elif args.config == "denoise":
             line = bench_denoise(args, ws, rank, local, dist)
+        elif args.config == "exposure":
+            line = bench_exposure(args, ws, rank, local, dist)
         else:
             line = bench_ours(args, ws, rank, local, dist)
         if line is not None:

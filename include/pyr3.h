@@ -154,6 +154,64 @@ int pyr3_read_histogram(pyr3_renderer *r, uint32_t *host_out);
  * histogram, computed on the device: width x height x RGBA f32 linear,
  * scene-referred values (k1, k2 from deriveCalibration, src/calibration.ts). */
 int pyr3_read_linear(pyr3_renderer *r, double k1, double k2, float *host_out);
+
+/* ---- auto-exposure ----------------------------------------------------- */
+/* Constants of src/auto-exposure.ts:43-61: the probe's long edge, quality
+ * and seed, the no-op deadband, the refinement cap and the brightness
+ * clamp. */
+#define PYR3_AE_PROBE_LONG_EDGE 1024
+#define PYR3_AE_PROBE_QUALITY 16
+#define PYR3_AE_PROBE_SEED 0x9e3779b9u
+#define PYR3_AE_DEADBAND 0.10
+#define PYR3_AE_MAX_ITERS 4
+#define PYR3_AE_BRIGHTNESS_MIN 1e-3
+#define PYR3_AE_BRIGHTNESS_MAX 1e4
+
+/* BrightnessFit (src/auto-exposure.ts:131-142). */
+typedef struct {
+  double brightness;  /* brightness to present the final image at */
+  int32_t corrected;  /* 1 iff brightness differs from the base */
+  int32_t iters;      /* re-presents performed */
+  double final_mean;  /* last measured mean luminance */
+  double factor;      /* target / initial mean (diagnostic) */
+} pyr3_brightness_fit;
+
+/* rerender(b, &mean, ctx): present at brightness b, store the measured mean
+ * luminance and return 0, or return a non-zero error code (which ends the
+ * fit and is returned). */
+typedef int (*pyr3_rerender_fn)(double brightness, double *mean, void *ctx);
+
+/* fitBrightnessToTarget (src/auto-exposure.ts:147-175), host logic only:
+ * fixed-point fit of the brightness so the measured mean luminance reaches
+ * target_mean, starting from initial_mean measured at base_brightness.
+ * No-op (fit->corrected = 0, no rerender call) inside the deadband or for a
+ * non-finite or non-positive target / initial mean. */
+int pyr3_fit_brightness(double base_brightness, double target_mean, double initial_mean,
+                        pyr3_rerender_fn rerender, void *ctx, pyr3_brightness_fit *fit);
+/* computeMeanLuminance / computeMeanLuminanceHalf (src/auto-exposure.ts:
+ * 70-97) of a DEVICE image of `pixels` RGBA pixels, on the renderer's
+ * stream; returns after the result is read back.  kind PYR3_OUT_RGBA8: mean
+ * of (R+G+B)/3 in [0, 255].  kind PYR3_OUT_RGBA32F: each channel rounded to
+ * binary16 (the rgba16float texture the reference reads back), non-finite
+ * -> 0, clamped to [0, 1], x 255.  0 pixels -> 0.  The image must be
+ * 16-byte aligned.  The sum is exact (integers on the device), so the mean
+ * is the same on every run. */
+int pyr3_mean_luminance(pyr3_renderer *r, const void *device_img, uint64_t pixels, int32_t kind,
+                        double *mean);
+/* The auto-exposure re-present loop of bin/pyr3-render.ts:487-513 on the
+ * device: present at p->brightness into device_out (W x H, out_kind),
+ * measure its mean luminance, then fitBrightnessToTarget with every
+ * re-present and measurement on the device (only the 8-byte luminance sum
+ * is read back per pass).  On return device_out holds the image at
+ * fit->brightness; k1 is derived from that brightness in double, as the
+ * reference's genome holds it.  target_mean comes from a probe render
+ * (measureProbeLuminance, src/auto-exposure.ts:99-129: the genome at
+ * PYR3_AE_PROBE_LONG_EDGE, PYR3_AE_PROBE_QUALITY spp, oversample 1, seed
+ * PYR3_AE_PROBE_SEED, measured with pyr3_mean_luminance). */
+int pyr3_auto_exposure(pyr3_renderer *r, const pyr3_present_opts *p, uint64_t total_samples,
+                       double target_mean, void *device_out, int32_t out_kind,
+                       pyr3_brightness_fit *fit);
+
 /* ---- batches ---------------------------------------------------------- */
 /* Batched rendering of many genomes (no counterpart in the reference,
  * which renders genomes one dispatch at a time): genomes too small to fill

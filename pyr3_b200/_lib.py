@@ -67,6 +67,15 @@ class PresentOpts(C.Structure):
                 ("hsl_hue", C.c_float), ("hsl_sat", C.c_float), ("hsl_light", C.c_float)]
 
 
+class BrightnessFit(C.Structure):
+    """pyr3_brightness_fit: BrightnessFit (src/auto-exposure.ts:131-142)."""
+    _fields_ = [("brightness", C.c_double), ("corrected", C.c_int32), ("iters", C.c_int32),
+                ("final_mean", C.c_double), ("factor", C.c_double)]
+
+
+# int rerender(double brightness, double *mean, void *ctx)
+RERENDER_FN = C.CFUNCTYPE(C.c_int, C.c_double, C.POINTER(C.c_double), C.c_void_p)
+
 # name -> (restype, argtypes)
 _SIGS = {
     "pyr3_create": (C.c_int, [C.POINTER(Opts), C.POINTER(C.c_void_p)]),
@@ -133,6 +142,12 @@ _SIGS = {
                                                C.c_void_p, C.c_int32, C.c_void_p]),
     "pyr3_prepare": (C.c_int, [C.c_void_p, C.POINTER(GenomeC)]),
     "pyr3_read_linear": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p]),
+    "pyr3_fit_brightness": (C.c_int, [C.c_double, C.c_double, C.c_double, RERENDER_FN, C.c_void_p,
+                                      C.POINTER(BrightnessFit)]),
+    "pyr3_mean_luminance": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32,
+                                      C.POINTER(C.c_double)]),
+    "pyr3_auto_exposure": (C.c_int, [C.c_void_p, C.POINTER(PresentOpts), C.c_uint64, C.c_double,
+                                     C.c_void_p, C.c_int32, C.POINTER(BrightnessFit)]),
     "pyr3_batch_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                     C.POINTER(C.c_void_p)]),
     "pyr3_batch_run": (C.c_int, [C.c_void_p]),

@@ -205,6 +205,8 @@ struct pyr3_renderer {
   size_t pick_cap = 0;
   uint64_t* d_counters = nullptr;
   uint64_t* d_sched = nullptr;  // queue kernel: [0] walkers handed out, [1] sticky fault flags
+  unsigned long long* d_luma = nullptr;  // luminance sum (auto-exposure)
+  unsigned long long* h_luma = nullptr;  // its pinned host copy
   uint32_t* d_wrec = nullptr;   // queue kernel: walker records (CTAs x slots)
   uint32_t* d_wave = nullptr;   // wave kernel: per population walker state + region counts
   size_t wave_bytes = 0;
@@ -302,6 +304,8 @@ PYR3_API int pyr3_create(const pyr3_opts* opts, pyr3_renderer** out) {
   CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, 16, r->stream));
   CUDA_TRY(cudaMalloc(&r->d_sched, 16));
   CUDA_TRY(cudaMemsetAsync(r->d_sched, 0, 16, r->stream));
+  CUDA_TRY(cudaMalloc(&r->d_luma, 8));
+  CUDA_TRY(cudaHostAlloc(&r->h_luma, 8, cudaHostAllocDefault));
   float knorm[257];
   kernel_norm_lut(knorm);
   CUDA_TRY(cudaMemcpyAsync(r->d_knorm, knorm, sizeof knorm, cudaMemcpyHostToDevice, r->stream));
@@ -329,6 +333,8 @@ PYR3_API int pyr3_destroy(pyr3_renderer* r) {
   cudaFree(r->d_pick);
   cudaFree(r->d_counters);
   cudaFree(r->d_sched);
+  cudaFree(r->d_luma);
+  cudaFreeHost(r->h_luma);
   cudaFree(r->d_wrec);
   cudaFree(r->d_wave);
   cudaFree(r->d_flush);
@@ -1122,14 +1128,16 @@ PYR3_API int pyr3_dn_adam(float* param, const float* grad, float* m, float* v, i
 }
 
 // ---------------------------------------------------------------- present
+// `brightness` replaces p->brightness: the auto-exposure loop presents at a
+// brightness it holds in double, as the reference's genome does.
 static int run_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t total_samples,
-                       void* dev_out, int32_t out_kind) {
+                       void* dev_out, int32_t out_kind, double brightness) {
   if (out_kind != PYR3_OUT_RGBA8 && out_kind != PYR3_OUT_RGBA32F)
     return fail(PYR3_E_INVALID, "unknown output kind");
   if (total_samples == 0) return fail(PYR3_E_INVALID, "total_samples must be positive");
   // src/calibration.ts:37-43 in double, uploaded as f32.
   const double os2 = (double)r->os * (double)r->os;
-  const float k1 = (float)((p->brightness * 255.0 * 268.0) / 256.0);
+  const float k1 = (float)((brightness * 255.0 * 268.0) / 256.0);
   const float k2 = (float)((os2 * p->scale * p->scale) / (255.0 * (double)total_samples));
   const float* filtered = nullptr;
   if (p->density_on) {
@@ -1178,7 +1186,7 @@ PYR3_API int pyr3_present_device(pyr3_renderer* r, const pyr3_present_opts* p,
                                  uint64_t total_samples, void* device_out, int32_t out_kind) {
   if (!r || !p || !device_out) return fail(PYR3_E_INVALID, "null argument");
   cudaSetDevice(r->device);
-  return run_present(r, p, total_samples, device_out, out_kind);
+  return run_present(r, p, total_samples, device_out, out_kind, p->brightness);
 }
 
 PYR3_API int pyr3_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t total_samples,
@@ -1188,11 +1196,105 @@ PYR3_API int pyr3_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t
   const size_t bytes = (size_t)r->W * r->H * (out_kind == PYR3_OUT_RGBA8 ? 4 : 16);
   int rc = ensure_out(r, bytes);
   if (rc) return rc;
-  rc = run_present(r, p, total_samples, r->d_out, out_kind);
+  rc = run_present(r, p, total_samples, r->d_out, out_kind, p->brightness);
   if (rc) return rc;
   CUDA_TRY(cudaMemcpyAsync(out, r->d_out, bytes, cudaMemcpyDeviceToHost, r->stream));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   return PYR3_OK;
+}
+
+// ------------------------------------------------------- auto-exposure
+namespace {
+// clamp of src/auto-exposure.ts:63-70: a non-finite value maps to lo.
+double ae_clamp(double x, double lo, double hi) {
+  return std::isfinite(x) ? std::min(hi, std::max(lo, x)) : lo;
+}
+
+// fitBrightnessToTarget (src/auto-exposure.ts:147-175); rerender(b, &mean)
+// returns 0 or an error code that ends the fit.
+template <class Rerender>
+int fit_brightness(double base, double target, double initial, Rerender&& rerender,
+                   pyr3_brightness_fit* fit) {
+  const bool finite = std::isfinite(target) && std::isfinite(initial);
+  const double factor0 = finite && initial > 0 ? target / initial : 1.0;
+  *fit = pyr3_brightness_fit{base, 0, 0, initial, factor0};
+  if (!finite || target <= 0 || initial <= 0 || std::fabs(factor0 - 1.0) <= PYR3_AE_DEADBAND)
+    return PYR3_OK;
+  double b = base, mean = initial;
+  int32_t iters = 0;
+  for (int k = 0; k < PYR3_AE_MAX_ITERS; ++k) {
+    const double factor = target / mean;
+    if (std::fabs(factor - 1.0) <= PYR3_AE_DEADBAND) break;
+    b = ae_clamp(b * factor, PYR3_AE_BRIGHTNESS_MIN, PYR3_AE_BRIGHTNESS_MAX);
+    const int rc = rerender(b, &mean);
+    if (rc) return rc;
+    ++iters;
+    if (mean <= 0) break;
+  }
+  fit->brightness = b;
+  fit->corrected = iters > 0;
+  fit->iters = iters;
+  fit->final_mean = mean;
+  return PYR3_OK;
+}
+
+// Mean luminance of a device image on the renderer's stream: an exact
+// integer sum on the device, then one division in double.
+int luma_mean(pyr3_renderer* r, const void* img, uint64_t pixels, int32_t kind, double* mean) {
+  if (pixels == 0) {
+    *mean = 0.0;  // computeMeanLuminance: empty -> 0
+    return PYR3_OK;
+  }
+  CUDA_TRY(cudaMemsetAsync(r->d_luma, 0, 8, r->stream));
+  CUDA_TRY(pyr3::launch_luma_sum(img, pixels, kind == PYR3_OUT_RGBA8, r->d_luma, device_sms(r->device),
+                                 r->stream));
+  CUDA_TRY(cudaMemcpyAsync(r->h_luma, r->d_luma, 8, cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  const double sum = (double)*r->h_luma, n = (double)pixels;
+  *mean = kind == PYR3_OUT_RGBA8 ? sum / (3.0 * n) : sum * 255.0 / (3.0 * 16777216.0 * n);
+  return PYR3_OK;
+}
+}  // namespace
+
+PYR3_API int pyr3_fit_brightness(double base_brightness, double target_mean, double initial_mean,
+                                 pyr3_rerender_fn rerender, void* ctx, pyr3_brightness_fit* fit) {
+  if (!rerender || !fit) return fail(PYR3_E_INVALID, "null argument");
+  return fit_brightness(base_brightness, target_mean, initial_mean,
+                        [&](double b, double* mean) -> int {
+                          const int rc = rerender(b, mean, ctx);
+                          return rc ? fail(rc, "fit_brightness: the rerender callback failed") : PYR3_OK;
+                        },
+                        fit);
+}
+
+PYR3_API int pyr3_mean_luminance(pyr3_renderer* r, const void* device_img, uint64_t pixels,
+                                 int32_t kind, double* mean) {
+  if (!r || !mean) return fail(PYR3_E_INVALID, "null argument");
+  if (kind != PYR3_OUT_RGBA8 && kind != PYR3_OUT_RGBA32F) return fail(PYR3_E_INVALID, "unknown image kind");
+  if (pixels && (!device_img || (uintptr_t)device_img % 16))
+    return fail(PYR3_E_INVALID, "the image must be a 16-byte aligned device buffer");
+  cudaSetDevice(r->device);
+  return luma_mean(r, device_img, pixels, kind, mean);
+}
+
+PYR3_API int pyr3_auto_exposure(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t total_samples,
+                                double target_mean, void* device_out, int32_t out_kind,
+                                pyr3_brightness_fit* fit) {
+  if (!r || !p || !device_out || !fit) return fail(PYR3_E_INVALID, "null argument");
+  if ((uintptr_t)device_out % 16) return fail(PYR3_E_INVALID, "device_out must be 16-byte aligned");
+  cudaSetDevice(r->device);
+  const uint64_t pixels = (uint64_t)r->W * r->H;
+  int rc = run_present(r, p, total_samples, device_out, out_kind, p->brightness);
+  if (rc) return rc;
+  double initial = 0.0;
+  rc = luma_mean(r, device_out, pixels, out_kind, &initial);
+  if (rc) return rc;
+  return fit_brightness(p->brightness, target_mean, initial,
+                        [&](double b, double* mean) -> int {
+                          const int e = run_present(r, p, total_samples, device_out, out_kind, b);
+                          return e ? e : luma_mean(r, device_out, pixels, out_kind, mean);
+                        },
+                        fit);
 }
 
 namespace {

@@ -19,8 +19,11 @@
 // for the raw histogram), flam3 alpha / vibrancy / highlight-power
 // composite, background blend, clamp, then the colour curves (5 x 256 LUT:
 // luma, r, g, b, composite, in the shader's order) and the HSL adjustment.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "passes.h"
 
@@ -215,47 +218,13 @@ __device__ __forceinline__ float curve_lut(const float* __restrict__ lut, int ch
   return lut[ch * 256 + i0] * (1.0f - t) + lut[ch * 256 + i1] * t;
 }
 
-template <bool kU32, bool kRgba8>
-__global__ void __launch_bounds__(256)
-k_tonemap(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapParams p,
-          const float* __restrict__ kern, const float* __restrict__ curves, void* __restrict__ out) {
-  __shared__ float kk[kMaxTaps];
-  if (threadIdx.x < p.fwidth) kk[threadIdx.x] = kern[threadIdx.x];
-  __syncthreads();
-  const uint32_t xi = blockIdx.x * 16 + (threadIdx.x & 15);
-  const uint32_t yi = blockIdx.y * 16 + (threadIdx.x >> 4);
-  if (xi >= p.width || yi >= p.height) return;
-  const int N = (int)p.oversample, fw = (int)p.fwidth, half = fw / 2;
-  const int sw = (int)p.width * N, sh = (int)p.height * N;
-  const int cx = (int)xi * N + N / 2, cy = (int)yi * N + N / 2;
-  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-  for (int dy = 0; dy < fw; ++dy) {
-    const float ky = kk[dy];
-    const int sy = min(max(cy + dy - half, 0), sh - 1);
-    for (int dx = 0; dx < fw; ++dx) {
-      const float kx = kk[dx];
-      const int sx = min(max(cx + dx - half, 0), sw - 1);
-      const size_t sb = (size_t)sy * sw + sx;
-      const float w = kx * ky;
-      if (kU32) {
-        const uint4 h = hu[sb];
-        const float cnt = (float)h.w;
-        if (cnt > 0.0f) {
-          const float ls = (p.k1 * logf(1.0f + cnt * p.k2)) / cnt;
-          s0 = s0 + ((float)h.x * ls) * w;
-          s1 = s1 + ((float)h.y * ls) * w;
-          s2 = s2 + ((float)h.z * ls) * w;
-          s3 = s3 + (cnt * ls) * w;
-        }
-      } else {
-        const float4 h = hf[sb];
-        s0 = s0 + h.x * w;
-        s1 = s1 + h.y * w;
-        s2 = s2 + h.z * w;
-        s3 = s3 + h.w * w;
-      }
-    }
-  }
+// The fragment tail of visualize (visualize_u32.wgsl:160-248): alpha,
+// vibrancy and highlight power from the filtered sums s0..s3, background,
+// colour curves, HSL; stored as rgba8 or rgba32f at pixel oi.
+template <bool kRgba8>
+__device__ __forceinline__ void tonemap_pixel(float s0, float s1, float s2, float s3,
+                                              const TonemapParams& p, const float* __restrict__ curves,
+                                              void* __restrict__ out, size_t oi) {
   float o[4];
   if (s3 <= 0.0f) {
     if (p.transparent) { o[0] = o[1] = o[2] = o[3] = 0.0f; }
@@ -304,7 +273,6 @@ k_tonemap(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapPa
     for (int i = 0; i < 3; ++i) o[i] = fminf(fmaxf(o[i], 0.0f), 1.0f);
     o[3] = p.transparent ? alpha : 1.0f;
   }
-  const size_t oi = (size_t)yi * p.width + xi;
   if (kRgba8) {
     uchar4 v;
     v.x = (unsigned char)__float2int_rn(o[0] * 255.0f);
@@ -315,6 +283,126 @@ k_tonemap(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapPa
   } else {
     ((float4*)out)[oi] = make_float4(o[0], o[1], o[2], o[3]);
   }
+}
+
+template <bool kU32, bool kRgba8>
+__global__ void __launch_bounds__(256)
+k_tonemap(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapParams p,
+          const float* __restrict__ kern, const float* __restrict__ curves, void* __restrict__ out) {
+  __shared__ float kk[kMaxTaps];
+  if (threadIdx.x < p.fwidth) kk[threadIdx.x] = kern[threadIdx.x];
+  __syncthreads();
+  const uint32_t xi = blockIdx.x * 16 + (threadIdx.x & 15);
+  const uint32_t yi = blockIdx.y * 16 + (threadIdx.x >> 4);
+  if (xi >= p.width || yi >= p.height) return;
+  const int N = (int)p.oversample, fw = (int)p.fwidth, half = fw / 2;
+  const int sw = (int)p.width * N, sh = (int)p.height * N;
+  const int cx = (int)xi * N + N / 2, cy = (int)yi * N + N / 2;
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+  for (int dy = 0; dy < fw; ++dy) {
+    const float ky = kk[dy];
+    const int sy = min(max(cy + dy - half, 0), sh - 1);
+    for (int dx = 0; dx < fw; ++dx) {
+      const float kx = kk[dx];
+      const int sx = min(max(cx + dx - half, 0), sw - 1);
+      const size_t sb = (size_t)sy * sw + sx;
+      const float w = kx * ky;
+      if (kU32) {
+        const uint4 h = hu[sb];
+        const float cnt = (float)h.w;
+        if (cnt > 0.0f) {
+          const float ls = (p.k1 * logf(1.0f + cnt * p.k2)) / cnt;
+          s0 = s0 + ((float)h.x * ls) * w;
+          s1 = s1 + ((float)h.y * ls) * w;
+          s2 = s2 + ((float)h.z * ls) * w;
+          s3 = s3 + (cnt * ls) * w;
+        }
+      } else {
+        const float4 h = hf[sb];
+        s0 = s0 + h.x * w;
+        s1 = s1 + h.y * w;
+        s2 = s2 + h.z * w;
+        s3 = s3 + h.w * w;
+      }
+    }
+  }
+  tonemap_pixel<kRgba8>(s0, s1, s2, s3, p, curves, out, (size_t)yi * p.width + xi);
+}
+
+// The same pass with the block's super-sampled tile staged in shared
+// memory: a block of T x T output pixels first reads the (T-1)N + fw square
+// of source buckets its filter taps cover (edge-clamped, coalesced rows),
+// converting each raw bucket to its log-density-scaled RGBA once, then
+// every pixel gathers its fw x fw taps from shared memory.  The taps are
+// added in the same order with the same products as k_tonemap, so the
+// output is the same bit for bit; each bucket is read from HBM once per
+// block instead of once per tap (about (fw/N)^2 times), and its logf is
+// taken once instead of per tap.
+template <bool kU32, bool kRgba8>
+__global__ void __launch_bounds__(256)
+k_tonemap_tile(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapParams p,
+               const float* __restrict__ kern, const float* __restrict__ curves, void* __restrict__ out,
+               int T, int side) {
+  extern __shared__ float4 tile[];  // side x side
+  __shared__ float kk[kMaxTaps];
+  if (threadIdx.x < p.fwidth) kk[threadIdx.x] = kern[threadIdx.x];
+  const int N = (int)p.oversample, fw = (int)p.fwidth, half = fw / 2;
+  const int sw = (int)p.width * N, sh = (int)p.height * N;
+  const int ox = (int)blockIdx.x * T * N + N / 2 - half, oy = (int)blockIdx.y * T * N + N / 2 - half;
+  // Four loads in flight per thread, then the conversions.
+  const int n = side * side, nt = (int)blockDim.x;
+  for (int e0 = threadIdx.x; e0 < n; e0 += 4 * nt) {
+    uint4 raw[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int e = e0 + j * nt;
+      if (e < n) {
+        const int ty = e / side, tx = e - ty * side;
+        const int sy = min(max(oy + ty, 0), sh - 1), sx = min(max(ox + tx, 0), sw - 1);
+        const size_t sb = (size_t)sy * sw + sx;
+        raw[j] = kU32 ? hu[sb] : reinterpret_cast<const uint4*>(hf)[sb];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int e = e0 + j * nt;
+      if (e >= n) break;
+      float4 v;
+      if (kU32) {
+        const uint4 h = raw[j];
+        const float cnt = (float)h.w;
+        if (cnt > 0.0f) {
+          const float ls = (p.k1 * logf(1.0f + cnt * p.k2)) / cnt;
+          v = make_float4((float)h.x * ls, (float)h.y * ls, (float)h.z * ls, cnt * ls);
+        } else {
+          v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // adds +0 to sums that are >= +0
+        }
+      } else {
+        v = make_float4(__uint_as_float(raw[j].x), __uint_as_float(raw[j].y), __uint_as_float(raw[j].z),
+                        __uint_as_float(raw[j].w));
+      }
+      tile[e] = v;
+    }
+  }
+  __syncthreads();
+  const int lx = (int)threadIdx.x % T, ly = (int)threadIdx.x / T;
+  const uint32_t xi = blockIdx.x * T + lx, yi = blockIdx.y * T + ly;
+  if (xi >= p.width || yi >= p.height) return;
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+  for (int dy = 0; dy < fw; ++dy) {
+    const float ky = kk[dy];
+    const float4* row = tile + (ly * N + dy) * side + lx * N;
+    for (int dx = 0; dx < fw; ++dx) {
+      const float kx = kk[dx];
+      const float w = kx * ky;
+      const float4 v = row[dx];
+      s0 = s0 + v.x * w;
+      s1 = s1 + v.y * w;
+      s2 = s2 + v.z * w;
+      s3 = s3 + v.w * w;
+    }
+  }
+  tonemap_pixel<kRgba8>(s0, s1, s2, s3, p, curves, out, (size_t)yi * p.width + xi);
 }
 
 // -------------------------------------------------------------- launch
@@ -335,6 +423,32 @@ cudaError_t launch_density(const uint32_t* hist, float* filtered, const DeParams
 cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, const TonemapParams& p,
                            const float* kern, const float* curves, void* out, bool rgba8,
                            cudaStream_t s) {
+  // Shared-memory tile of 16 x 16 (else 8 x 8) output pixels when its source
+  // square fits in 48 KB; the per-tap gather otherwise (large oversample
+  // with a wide filter).
+  const int N = (int)p.oversample, fw = (int)p.fwidth;
+  int T = 0, side = 0;
+  for (int t : {16, 8}) {
+    const int sd = (t - 1) * N + fw;
+    if ((size_t)sd * sd * sizeof(float4) <= 48 * 1024) {
+      T = t;
+      side = sd;
+      break;
+    }
+  }
+  if (T) {
+    dim3 grid((p.width + T - 1) / T, (p.height + T - 1) / T);
+    const size_t smem = (size_t)side * side * sizeof(float4);
+    const unsigned thr = (unsigned)(T * T);
+    if (hist_u32) {
+      if (rgba8) k_tonemap_tile<true, true><<<grid, thr, smem, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out, T, side);
+      else k_tonemap_tile<true, false><<<grid, thr, smem, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out, T, side);
+    } else {
+      if (rgba8) k_tonemap_tile<false, true><<<grid, thr, smem, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out, T, side);
+      else k_tonemap_tile<false, false><<<grid, thr, smem, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out, T, side);
+    }
+    return cudaGetLastError();
+  }
   dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
   if (hist_u32) {
     if (rgba8) k_tonemap<true, true><<<grid, 256, 0, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out);
@@ -401,6 +515,75 @@ __global__ void __launch_bounds__(256) k_splat_rate(uint32_t* cells, uint64_t n_
 cudaError_t launch_splat_rate(uint32_t* cells, uint64_t n_cells, uint64_t splats, int sms, cudaStream_t s) {
   const uint64_t threads = (uint64_t)sms * 8 * 256;
   k_splat_rate<<<(unsigned)(sms * 8), 256, 0, s>>>(cells, n_cells, splats / threads, splats % threads);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ luminance
+namespace {
+__device__ __forceinline__ uint32_t rgb8_sum(uint32_t px) {
+  return (px & 0xffu) + ((px >> 8) & 0xffu) + ((px >> 16) & 0xffu);
+}
+
+// One channel of an rgba32f pixel as the reference reads it back from an
+// rgba16float texture: rounded to binary16, non-finite -> 0, clamped to
+// [0, 1]; in units of 2^-24.
+__device__ __forceinline__ uint32_t half_units(float x) {
+  const float h = __half2float(__float2half_rn(x));
+  if (!(fabsf(h) <= 65504.0f)) return 0u;
+  return (uint32_t)(fminf(fmaxf(h, 0.0f), 1.0f) * 16777216.0f);
+}
+
+// Grid-stride over 16-byte words (4 rgba8 pixels or 1 rgba32f pixel), four
+// independent loads in flight per thread; one atomic per block.
+template <bool RGBA8>
+__global__ void __launch_bounds__(256) k_luma_sum(const uint4* __restrict__ img, uint64_t words,
+                                                  const uint32_t* __restrict__ tail, uint32_t n_tail,
+                                                  unsigned long long* sum) {
+  const uint64_t stride = (uint64_t)gridDim.x * 256;
+  uint64_t acc = 0;
+  uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
+  auto add = [&](const uint4 v) {
+    if (RGBA8)
+      acc += rgb8_sum(v.x) + rgb8_sum(v.y) + rgb8_sum(v.z) + rgb8_sum(v.w);
+    else
+      acc += half_units(__uint_as_float(v.x)) + half_units(__uint_as_float(v.y)) +
+             half_units(__uint_as_float(v.z));
+  };
+  for (; i + 3 * stride < words; i += 4 * stride) {
+    const uint4 a = __ldcs(img + i), b = __ldcs(img + i + stride), c = __ldcs(img + i + 2 * stride),
+                d = __ldcs(img + i + 3 * stride);
+    add(a);
+    add(b);
+    add(c);
+    add(d);
+  }
+  for (; i < words; i += stride) add(__ldcs(img + i));
+  if (RGBA8 && blockIdx.x == 0 && threadIdx.x < n_tail) acc += rgb8_sum(tail[threadIdx.x]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  __shared__ uint64_t warp_sums[8];
+  if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t t = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) t += warp_sums[w];
+    atomicAdd(sum, (unsigned long long)t);
+  }
+}
+}  // namespace
+
+cudaError_t launch_luma_sum(const void* img, uint64_t pixels, bool rgba8, unsigned long long* sum,
+                            int sms, cudaStream_t s) {
+  const uint64_t words = rgba8 ? pixels / 4 : pixels;
+  const uint32_t n_tail = rgba8 ? (uint32_t)(pixels % 4) : 0u;
+  const uint64_t want = (words + 255) / 256;
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sms * 8));
+  const uint32_t* tail = (const uint32_t*)img + words * 4;
+  if (rgba8)
+    k_luma_sum<true><<<grid, 256, 0, s>>>((const uint4*)img, words, tail, n_tail, sum);
+  else
+    k_luma_sum<false><<<grid, 256, 0, s>>>((const uint4*)img, words, nullptr, 0, sum);
   return cudaGetLastError();
 }
 }  // namespace pyr3

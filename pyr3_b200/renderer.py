@@ -172,6 +172,16 @@ class Renderer:
         _lib.check(_lib.lib().pyr3_present(self._h, C.byref(p), int(total_samples), _lib.ptr(out), kind))
         return out
 
+    def present_device(self, genome: Genome, total_samples: int, device_out: int,
+                       force_de_off: bool = False, transparent: bool = False,
+                       fmt: str = "rgba8") -> None:
+        """present() into a device buffer (a pointer to W x H RGBA u8 or f32,
+        e.g. a CUDA tensor's data_ptr()), queued on the renderer's stream."""
+        kind = _lib.OUT_RGBA8 if fmt == "rgba8" else _lib.OUT_RGBA32F
+        p = self.present_opts(genome, force_de_off, transparent)
+        _lib.check(_lib.lib().pyr3_present_device(self._h, C.byref(p), int(total_samples),
+                                                  C.c_void_p(int(device_out)), kind))
+
     def render(self, genome: Genome, seed: int = 0, **kw) -> np.ndarray:
         """reset + iterate + present (src/renderer.ts:264-278)."""
         spp = genome.quality if genome.quality is not None else DEFAULT_SPP

@@ -269,6 +269,36 @@ def test_density_tonemap_within_1_255(os_, de):
     assert float(np.abs(out - ref).max()) <= 1.0 / 255.0
 
 
+@pytest.mark.parametrize("os_,radius", [(1, 0.5), (2, 0.5), (3, 2.0), (8, 2.0)])
+def test_tonemap_tile_paths_within_1_255(os_, radius):
+    """The tonemap's three launch shapes -- a 16 x 16 shared-memory tile
+    (oversample 1 and 2), an 8 x 8 tile (oversample 3, 17 taps) and the
+    per-tap gather (oversample 8, 17 taps: the tile would not fit in 48 KB)
+    -- on a ragged 37 x 29 canvas of random buckets, a quarter of them
+    empty, against the oracle's visualize."""
+    W, H = 37, 29
+    rng = np.random.default_rng(os_)
+    n = W * os_ * H * os_
+    cnt = rng.integers(0, 1000, n).astype(np.uint32)
+    cnt[rng.random(n) < 0.25] = 0
+    hist = np.zeros((n, 4), np.uint32)
+    hist[:, 3] = cnt * 255
+    for c in range(3):
+        hist[:, c] = (cnt * rng.integers(0, 256, n)).astype(np.uint32)
+    hist = hist.reshape(-1)
+    g = workloads.plain_small()
+    g.scale = W / 4
+    samples = int(cnt.sum())
+    p = R.Renderer.present_opts(None, g, force_de_off=True)
+    out = np.zeros(W * H * 4, np.float32)
+    _lib.check(_lib.lib().pyr3_density_tonemap(_lib.ptr(hist), W, H, os_, radius, C.byref(p), samples,
+                                               _lib.ptr(out), None))
+    k1, k2 = O.derive_calibration(g.scale, samples, 4.0, os_)
+    ref = O.visualize(W, H, os_, O.spatial_kernel(radius, os_), np.float32(k1), np.float32(k2), 4.0, 1.0,
+                      1.0, 0.01, src_u32=hist)
+    assert float(np.abs(out - ref).max()) <= 1.0 / 255.0
+
+
 def test_tonemap_curves_and_hsl_within_1_255():
     """Colour curves (composite, r, b, luma) + HSL adjustment on a DE'd
     histogram: device tonemap vs the oracle's visualize within 1/255."""
