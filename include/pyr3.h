@@ -117,6 +117,13 @@ typedef struct {
 
 #define PYR3_OUT_RGBA8 0      /* W x H x 4 u8 (rgba8unorm) */
 #define PYR3_OUT_RGBA32F 1    /* W x H x 4 f32 (fragment value) */
+#define PYR3_OUT_RGBA16F 2    /* W x H x 4 binary16, nearest even (the rgba16float
+                                 texture of the png16 and exr exports) */
+#define PYR3_OUT_PNG16 3      /* W x H x 4 u16: displayHalfToPng16
+                                 (src/gpu-readback.ts:106-115) of the rgba16float value */
+#define PYR3_OUT_EXR_DISPLAY 4 /* W x H x 4 f32: displayHalfToLinearExr
+                                 (src/gpu-readback.ts:83-104): sRGB-to-linear RGB of
+                                 the clamped rgba16float value, alpha clamped */
 
 typedef struct pyr3_batch pyr3_batch;
 
@@ -139,8 +146,11 @@ int pyr3_reset(pyr3_renderer *r, const float *palette);
 int pyr3_iterate(pyr3_renderer *r, const pyr3_genome *g, const pyr3_iterate_opts *o);
 /* Renderer.present (src/renderer.ts:241): density estimation (optional) +
  * tonemap of the accumulated histogram.  total_samples = sum of
- * walkers*iters since reset.  `out` is a HOST buffer of W*H*4 u8 or f32
- * per out_kind; the call returns after the copy. */
+ * walkers*iters since reset.  `out` is a HOST buffer of W*H pixels of
+ * out_kind (PYR3_OUT_*: 4, 16, 8, 8 or 16 bytes each); the call returns
+ * after the copy.  The png16 and exr kinds are written by the tonemap pass
+ * itself, in place of the reference's host-side transforms of its
+ * rgba16float readback. */
 int pyr3_present(pyr3_renderer *r, const pyr3_present_opts *p, uint64_t total_samples,
                  void *out, int32_t out_kind);
 /* Same as pyr3_present but writes into a DEVICE buffer and returns without
@@ -154,6 +164,13 @@ int pyr3_read_histogram(pyr3_renderer *r, uint32_t *host_out);
  * histogram, computed on the device: width x height x RGBA f32 linear,
  * scene-referred values (k1, k2 from deriveCalibration, src/calibration.ts). */
 int pyr3_read_linear(pyr3_renderer *r, double k1, double k2, float *host_out);
+/* An rgba32f fragment-value image already on the device (e.g. from
+ * pyr3_present_device) written as another output kind, with the same
+ * per-pixel steps as the tonemap's store: one present can feed several
+ * exports.  Both buffers 16-byte aligned; runs on `stream` (a cudaStream_t,
+ * NULL = default stream) of the current device. */
+int pyr3_convert_display(const void *device_rgba32f, uint64_t pixels, int32_t out_kind,
+                         void *device_out, void *stream);
 
 /* ---- auto-exposure ----------------------------------------------------- */
 /* Constants of src/auto-exposure.ts:43-61: the probe's long edge, quality
@@ -191,15 +208,17 @@ int pyr3_fit_brightness(double base_brightness, double target_mean, double initi
 /* computeMeanLuminance / computeMeanLuminanceHalf (src/auto-exposure.ts:
  * 70-97) of a DEVICE image of `pixels` RGBA pixels, on the renderer's
  * stream; returns after the result is read back.  kind PYR3_OUT_RGBA8: mean
- * of (R+G+B)/3 in [0, 255].  kind PYR3_OUT_RGBA32F: each channel rounded to
- * binary16 (the rgba16float texture the reference reads back), non-finite
- * -> 0, clamped to [0, 1], x 255.  0 pixels -> 0.  The image must be
- * 16-byte aligned.  The sum is exact (integers on the device), so the mean
+ * of (R+G+B)/3 in [0, 255].  kind PYR3_OUT_RGBA16F: computeMeanLuminanceHalf
+ * (non-finite -> 0, clamped to [0, 1], x 255).  kind PYR3_OUT_RGBA32F: the
+ * same after rounding each channel to binary16 (the rgba16float texture
+ * the reference reads back).  0 pixels -> 0.  The image must be 16-byte
+ * aligned.  The sum is exact (integers on the device), so the mean
  * is the same on every run. */
 int pyr3_mean_luminance(pyr3_renderer *r, const void *device_img, uint64_t pixels, int32_t kind,
                         double *mean);
 /* The auto-exposure re-present loop of bin/pyr3-render.ts:487-513 on the
- * device: present at p->brightness into device_out (W x H, out_kind),
+ * device: present at p->brightness into device_out (W x H, out_kind
+ * PYR3_OUT_RGBA8, PYR3_OUT_RGBA16F or PYR3_OUT_RGBA32F),
  * measure its mean luminance, then fitBrightnessToTarget with every
  * re-present and measurement on the device (only the 8-byte luminance sum
  * is read back per pass).  On return device_out holds the image at
@@ -298,7 +317,7 @@ int pyr3_density_tonemap(const uint32_t *hist, uint32_t width, uint32_t height,
  * inside another engine's frame loop or memory pool, or code that must not
  * allocate once running.  The caller passes a super-res histogram already
  * on the device (superW x superH x 4 u32) and a device output image
- * (width x height, PYR3_OUT_RGBA8 or PYR3_OUT_RGBA32F); the intermediate
+ * (width x height, any PYR3_OUT_* kind); the intermediate
  * density output and lookup tables live in one fixed array inside the
  * library (about 16.4 MiB, held by every GPU that loads the library until
  * the process exits).  Limit: width*height*oversample^2 <= 1,048,576

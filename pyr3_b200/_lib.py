@@ -22,6 +22,9 @@ PYR3_E_NOMEM = -4
 PYR3_E_UNSUPPORTED = -5
 OUT_RGBA8 = 0
 OUT_RGBA32F = 1
+OUT_RGBA16F = 2
+OUT_PNG16 = 3
+OUT_EXR_DISPLAY = 4
 ITER_EXACT_WALKERS = 1
 ITER_AGGREGATE = 2
 ITER_KERNEL_BARRIER = 4
@@ -142,6 +145,7 @@ _SIGS = {
                                                C.c_void_p, C.c_int32, C.c_void_p]),
     "pyr3_prepare": (C.c_int, [C.c_void_p, C.POINTER(GenomeC)]),
     "pyr3_read_linear": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p]),
+    "pyr3_convert_display": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p, C.c_void_p]),
     "pyr3_fit_brightness": (C.c_int, [C.c_double, C.c_double, C.c_double, RERENDER_FN, C.c_void_p,
                                       C.POINTER(BrightnessFit)]),
     "pyr3_mean_luminance": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32,

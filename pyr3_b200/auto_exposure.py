@@ -88,13 +88,16 @@ def _kind(image) -> int:
         return _lib.OUT_RGBA8
     if image.dtype == torch.float32:
         return _lib.OUT_RGBA32F
-    raise ValueError("image must be RGBA uint8 or float32")
+    if image.dtype == torch.float16:
+        return _lib.OUT_RGBA16F
+    raise ValueError("image must be RGBA uint8, float16 or float32")
 
 
 def mean_luminance(renderer: Renderer, image) -> float:
     """computeMeanLuminance / computeMeanLuminanceHalf (src/auto-exposure.ts:
-    70-97) of an RGBA CUDA tensor (uint8: rgba8unorm; float32: read as the
-    rgba16float texture the reference measures), computed on the device."""
+    70-97) of an RGBA CUDA tensor (uint8: rgba8unorm; float16: the
+    rgba16float texture; float32: read as that texture), computed on the
+    device."""
     if not image.is_cuda or not image.is_contiguous() or image.numel() % 4:
         raise ValueError("image must be a contiguous RGBA CUDA tensor")
     _after_torch(image)
@@ -167,14 +170,16 @@ def auto_expose(renderer: Renderer, genome: Genome, total_samples: int, target_m
                 image=None, fmt: str = "rgba8", force_de_off: bool = False,
                 transparent: bool = False):
     """The re-present loop of bin/pyr3-render.ts:487-513 on the device:
-    present at the genome's brightness, measure, refine.  Returns the fit
-    and the CUDA image (H x W x 4, uint8 or float32) at fit.brightness."""
+    present at the genome's brightness, measure, refine.  fmt "rgba8", "f16"
+    (the rgba16float texture of the png16 / exr exports) or "f32".  Returns
+    the fit and the CUDA image (H x W x 4) at fit.brightness."""
     import torch
 
-    kind = _lib.OUT_RGBA8 if fmt == "rgba8" else _lib.OUT_RGBA32F
+    kind = {"rgba8": _lib.OUT_RGBA8, "f32": _lib.OUT_RGBA32F, "f16": _lib.OUT_RGBA16F}[fmt]
     if image is None:
-        image = torch.empty((renderer.height, renderer.width, 4),
-                            dtype=torch.uint8 if kind == _lib.OUT_RGBA8 else torch.float32,
+        dtype = {_lib.OUT_RGBA8: torch.uint8, _lib.OUT_RGBA32F: torch.float32,
+                 _lib.OUT_RGBA16F: torch.float16}[kind]
+        image = torch.empty((renderer.height, renderer.width, 4), dtype=dtype,
                             device=torch.device("cuda", renderer._opts.device))
     elif _kind(image) != kind or image.numel() != renderer.width * renderer.height * 4:
         raise ValueError("image does not match the renderer's size and format")

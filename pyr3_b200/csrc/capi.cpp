@@ -1132,8 +1132,7 @@ PYR3_API int pyr3_dn_adam(float* param, const float* grad, float* m, float* v, i
 // brightness it holds in double, as the reference's genome does.
 static int run_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t total_samples,
                        void* dev_out, int32_t out_kind, double brightness) {
-  if (out_kind != PYR3_OUT_RGBA8 && out_kind != PYR3_OUT_RGBA32F)
-    return fail(PYR3_E_INVALID, "unknown output kind");
+  if (pyr3::out_bytes_per_pixel(out_kind) == 0) return fail(PYR3_E_INVALID, "unknown output kind");
   if (total_samples == 0) return fail(PYR3_E_INVALID, "total_samples must be positive");
   // src/calibration.ts:37-43 in double, uploaded as f32.
   const double os2 = (double)r->os * (double)r->os;
@@ -1178,7 +1177,7 @@ static int run_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t to
   t.hsl_sat = p->hsl_sat;
   t.hsl_light = p->hsl_light;
   CUDA_TRY(pyr3::launch_tonemap(filtered ? nullptr : r->d_hist, filtered, t, r->d_kern, r->d_curves,
-                                dev_out, out_kind == PYR3_OUT_RGBA8, r->stream));
+                                dev_out, out_kind, r->stream));
   return PYR3_OK;
 }
 
@@ -1193,7 +1192,9 @@ PYR3_API int pyr3_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t
                           void* out, int32_t out_kind) {
   if (!r || !p || !out) return fail(PYR3_E_INVALID, "null argument");
   cudaSetDevice(r->device);
-  const size_t bytes = (size_t)r->W * r->H * (out_kind == PYR3_OUT_RGBA8 ? 4 : 16);
+  const size_t bpp = pyr3::out_bytes_per_pixel(out_kind);
+  if (bpp == 0) return fail(PYR3_E_INVALID, "unknown output kind");
+  const size_t bytes = (size_t)r->W * r->H * bpp;
   int rc = ensure_out(r, bytes);
   if (rc) return rc;
   rc = run_present(r, p, total_samples, r->d_out, out_kind, p->brightness);
@@ -1246,8 +1247,7 @@ int luma_mean(pyr3_renderer* r, const void* img, uint64_t pixels, int32_t kind, 
     return PYR3_OK;
   }
   CUDA_TRY(cudaMemsetAsync(r->d_luma, 0, 8, r->stream));
-  CUDA_TRY(pyr3::launch_luma_sum(img, pixels, kind == PYR3_OUT_RGBA8, r->d_luma, device_sms(r->device),
-                                 r->stream));
+  CUDA_TRY(pyr3::launch_luma_sum(img, pixels, kind, r->d_luma, device_sms(r->device), r->stream));
   CUDA_TRY(cudaMemcpyAsync(r->h_luma, r->d_luma, 8, cudaMemcpyDeviceToHost, r->stream));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   const double sum = (double)*r->h_luma, n = (double)pixels;
@@ -1270,11 +1270,25 @@ PYR3_API int pyr3_fit_brightness(double base_brightness, double target_mean, dou
 PYR3_API int pyr3_mean_luminance(pyr3_renderer* r, const void* device_img, uint64_t pixels,
                                  int32_t kind, double* mean) {
   if (!r || !mean) return fail(PYR3_E_INVALID, "null argument");
-  if (kind != PYR3_OUT_RGBA8 && kind != PYR3_OUT_RGBA32F) return fail(PYR3_E_INVALID, "unknown image kind");
+  if (kind != PYR3_OUT_RGBA8 && kind != PYR3_OUT_RGBA32F && kind != PYR3_OUT_RGBA16F)
+    return fail(PYR3_E_INVALID, "mean luminance: the image must be rgba8, rgba32f or rgba16f");
   if (pixels && (!device_img || (uintptr_t)device_img % 16))
     return fail(PYR3_E_INVALID, "the image must be a 16-byte aligned device buffer");
   cudaSetDevice(r->device);
   return luma_mean(r, device_img, pixels, kind, mean);
+}
+
+PYR3_API int pyr3_convert_display(const void* device_rgba32f, uint64_t pixels, int32_t out_kind,
+                                  void* device_out, void* stream) {
+  if (pyr3::out_bytes_per_pixel(out_kind) == 0) return fail(PYR3_E_INVALID, "unknown output kind");
+  if (pixels && (!device_rgba32f || !device_out || (uintptr_t)device_rgba32f % 16 ||
+                 (uintptr_t)device_out % 16))
+    return fail(PYR3_E_INVALID, "convert_display: images must be 16-byte aligned device buffers");
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(pyr3::launch_convert_display((const float*)device_rgba32f, pixels, out_kind, device_out,
+                                        device_sms(dev), (cudaStream_t)stream));
+  return PYR3_OK;
 }
 
 PYR3_API int pyr3_auto_exposure(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t total_samples,
@@ -1282,6 +1296,8 @@ PYR3_API int pyr3_auto_exposure(pyr3_renderer* r, const pyr3_present_opts* p, ui
                                 pyr3_brightness_fit* fit) {
   if (!r || !p || !device_out || !fit) return fail(PYR3_E_INVALID, "null argument");
   if ((uintptr_t)device_out % 16) return fail(PYR3_E_INVALID, "device_out must be 16-byte aligned");
+  if (out_kind != PYR3_OUT_RGBA8 && out_kind != PYR3_OUT_RGBA32F && out_kind != PYR3_OUT_RGBA16F)
+    return fail(PYR3_E_INVALID, "auto-exposure measures rgba8, rgba32f or rgba16f images");
   cudaSetDevice(r->device);
   const uint64_t pixels = (uint64_t)r->W * r->H;
   int rc = run_present(r, p, total_samples, device_out, out_kind, p->brightness);
@@ -1574,8 +1590,7 @@ PYR3_API int pyr3_density_tonemap_noalloc(const uint32_t* device_hist, uint32_t 
                                           int32_t out_kind, void* stream) {
   if (!device_hist || !p || !device_out || oversample == 0 || width == 0 || height == 0)
     return fail(PYR3_E_INVALID, "bad arguments");
-  if (out_kind != PYR3_OUT_RGBA8 && out_kind != PYR3_OUT_RGBA32F)
-    return fail(PYR3_E_INVALID, "unknown output kind");
+  if (pyr3::out_bytes_per_pixel(out_kind) == 0) return fail(PYR3_E_INVALID, "unknown output kind");
   if (total_samples == 0) return fail(PYR3_E_INVALID, "total_samples must be positive");
   const uint64_t sw = (uint64_t)width * oversample, sh = (uint64_t)height * oversample;
   if (sw * sh > pyr3::kNoAllocMaxSuperPixels)
@@ -1633,7 +1648,7 @@ PYR3_API int pyr3_density_tonemap_noalloc(const uint32_t* device_hist, uint32_t 
   t.hsl_sat = p->hsl_sat;
   t.hsl_light = p->hsl_light;
   CUDA_TRY(pyr3::launch_tonemap(filtered ? nullptr : device_hist, filtered, t, sc.kern, sc.curves,
-                                device_out, out_kind == PYR3_OUT_RGBA8, s));
+                                device_out, out_kind, s));
   return PYR3_OK;
 }
 

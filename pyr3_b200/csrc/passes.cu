@@ -218,10 +218,70 @@ __device__ __forceinline__ float curve_lut(const float* __restrict__ lut, int ch
   return lut[ch * 256 + i0] * (1.0f - t) + lut[ch * 256 + i1] * t;
 }
 
+// ------------------------------------------------------- output kinds
+// The display texture the reference renders to is rgba8unorm or
+// rgba16float; its png16 and EXR exports transform the rgba16float readback
+// on the host (src/gpu-readback.ts:83-115).  Here every kind is written by
+// the pass that produces the fragment value.
+__device__ __forceinline__ float to_half(float x) { return __half2float(__float2half_rn(x)); }
+
+// displayHalfToPng16 (src/gpu-readback.ts:106-115) of one channel:
+// round(clamp(h, 0, 1) * 65535), NaN -> 0.  Every binary16 in [0, 1] is
+// k * 2^-24 with integer k, so the rounding is exact integer arithmetic:
+// floor(k * 65535 / 2^24 + 1/2).
+__device__ __forceinline__ uint16_t png16_sample(float x) {
+  const float h = to_half(x);
+  if (h != h) return 0;
+  const uint64_t k = (uint64_t)(fminf(fmaxf(h, 0.0f), 1.0f) * 16777216.0f);
+  return (uint16_t)((k * 65535ull + (1ull << 23)) >> 24);
+}
+
+// The clamp of displayHalfToLinearExr (src/gpu-readback.ts:90-93):
+// non-finite -> 0, else clamp to [0, 1]; -0 becomes +0, as JS Math.max(0, -0)
+// does (the + 0.0f).
+__device__ __forceinline__ float exr_clamp(float x) {
+  const float h = to_half(x);
+  return fabsf(h) <= 65504.0f ? fminf(fmaxf(h, 0.0f), 1.0f) + 0.0f : 0.0f;
+}
+
+// srgbToLinear (src/srgb.ts:13-16) in double, as the reference computes
+// it, rounded to f32 (its Float32Array).
+__device__ __forceinline__ float srgb_to_linear(float c) {
+  const double d = (double)c;
+  return (float)(d <= 0.04045 ? d / 12.92 : pow((d + 0.055) / 1.055, 2.4));
+}
+
+template <int kOut>
+__device__ __forceinline__ void store_pixel(const float o[4], void* __restrict__ out, size_t oi) {
+  if (kOut == kOutRgba8) {
+    uchar4 v;
+    v.x = (unsigned char)__float2int_rn(o[0] * 255.0f);
+    v.y = (unsigned char)__float2int_rn(o[1] * 255.0f);
+    v.z = (unsigned char)__float2int_rn(o[2] * 255.0f);
+    v.w = (unsigned char)__float2int_rn(o[3] * 255.0f);
+    ((uchar4*)out)[oi] = v;
+  } else if (kOut == kOutRgba32f) {
+    ((float4*)out)[oi] = make_float4(o[0], o[1], o[2], o[3]);
+  } else if (kOut == kOutRgba16f) {
+    ushort4 v;
+    v.x = __half_as_ushort(__float2half_rn(o[0]));
+    v.y = __half_as_ushort(__float2half_rn(o[1]));
+    v.z = __half_as_ushort(__float2half_rn(o[2]));
+    v.w = __half_as_ushort(__float2half_rn(o[3]));
+    ((ushort4*)out)[oi] = v;
+  } else if (kOut == kOutPng16) {
+    ((ushort4*)out)[oi] = make_ushort4(png16_sample(o[0]), png16_sample(o[1]), png16_sample(o[2]),
+                                       png16_sample(o[3]));
+  } else {  // kOutExrDisplay
+    ((float4*)out)[oi] = make_float4(srgb_to_linear(exr_clamp(o[0])), srgb_to_linear(exr_clamp(o[1])),
+                                     srgb_to_linear(exr_clamp(o[2])), exr_clamp(o[3]));
+  }
+}
+
 // The fragment tail of visualize (visualize_u32.wgsl:160-248): alpha,
 // vibrancy and highlight power from the filtered sums s0..s3, background,
-// colour curves, HSL; stored as rgba8 or rgba32f at pixel oi.
-template <bool kRgba8>
+// colour curves, HSL; stored at pixel oi as output kind kOut.
+template <int kOut>
 __device__ __forceinline__ void tonemap_pixel(float s0, float s1, float s2, float s3,
                                               const TonemapParams& p, const float* __restrict__ curves,
                                               void* __restrict__ out, size_t oi) {
@@ -273,19 +333,10 @@ __device__ __forceinline__ void tonemap_pixel(float s0, float s1, float s2, floa
     for (int i = 0; i < 3; ++i) o[i] = fminf(fmaxf(o[i], 0.0f), 1.0f);
     o[3] = p.transparent ? alpha : 1.0f;
   }
-  if (kRgba8) {
-    uchar4 v;
-    v.x = (unsigned char)__float2int_rn(o[0] * 255.0f);
-    v.y = (unsigned char)__float2int_rn(o[1] * 255.0f);
-    v.z = (unsigned char)__float2int_rn(o[2] * 255.0f);
-    v.w = (unsigned char)__float2int_rn(o[3] * 255.0f);
-    ((uchar4*)out)[oi] = v;
-  } else {
-    ((float4*)out)[oi] = make_float4(o[0], o[1], o[2], o[3]);
-  }
+  store_pixel<kOut>(o, out, oi);
 }
 
-template <bool kU32, bool kRgba8>
+template <bool kU32, int kOut>
 __global__ void __launch_bounds__(256)
 k_tonemap(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapParams p,
           const float* __restrict__ kern, const float* __restrict__ curves, void* __restrict__ out) {
@@ -326,7 +377,7 @@ k_tonemap(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapPa
       }
     }
   }
-  tonemap_pixel<kRgba8>(s0, s1, s2, s3, p, curves, out, (size_t)yi * p.width + xi);
+  tonemap_pixel<kOut>(s0, s1, s2, s3, p, curves, out, (size_t)yi * p.width + xi);
 }
 
 // The same pass with the block's super-sampled tile staged in shared
@@ -338,7 +389,7 @@ k_tonemap(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapPa
 // output is the same bit for bit; each bucket is read from HBM once per
 // block instead of once per tap (about (fw/N)^2 times), and its logf is
 // taken once instead of per tap.
-template <bool kU32, bool kRgba8>
+template <bool kU32, int kOut>
 __global__ void __launch_bounds__(256)
 k_tonemap_tile(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapParams p,
                const float* __restrict__ kern, const float* __restrict__ curves, void* __restrict__ out,
@@ -402,7 +453,7 @@ k_tonemap_tile(const uint4* __restrict__ hu, const float4* __restrict__ hf, Tone
       s3 = s3 + v.w * w;
     }
   }
-  tonemap_pixel<kRgba8>(s0, s1, s2, s3, p, curves, out, (size_t)yi * p.width + xi);
+  tonemap_pixel<kOut>(s0, s1, s2, s3, p, curves, out, (size_t)yi * p.width + xi);
 }
 
 // -------------------------------------------------------------- launch
@@ -420,8 +471,51 @@ cudaError_t launch_density(const uint32_t* hist, float* filtered, const DeParams
   return cudaGetLastError();
 }
 
+namespace {
+template <int kOut>
+void tonemap_launch(const uint32_t* hist_u32, const float* filtered, const TonemapParams& p,
+                    const float* kern, const float* curves, void* out, int T, int side, cudaStream_t s) {
+  if (T) {
+    dim3 grid((p.width + T - 1) / T, (p.height + T - 1) / T);
+    const size_t smem = (size_t)side * side * sizeof(float4);
+    const unsigned thr = (unsigned)(T * T);
+    if (hist_u32)
+      k_tonemap_tile<true, kOut><<<grid, thr, smem, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out, T, side);
+    else
+      k_tonemap_tile<false, kOut><<<grid, thr, smem, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out, T, side);
+    return;
+  }
+  dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
+  if (hist_u32)
+    k_tonemap<true, kOut><<<grid, 256, 0, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out);
+  else
+    k_tonemap<false, kOut><<<grid, 256, 0, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out);
+}
+
+template <int kOut>
+__global__ void __launch_bounds__(256) k_convert_display(const float4* __restrict__ in, uint64_t n,
+                                                         void* __restrict__ out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (uint64_t)gridDim.x * 256) {
+    const float4 v = in[i];
+    const float o[4] = {v.x, v.y, v.z, v.w};
+    store_pixel<kOut>(o, out, i);
+  }
+}
+}  // namespace
+
+size_t out_bytes_per_pixel(int out_kind) {
+  switch (out_kind) {
+    case kOutRgba8: return 4;
+    case kOutRgba16f:
+    case kOutPng16: return 8;
+    case kOutRgba32f:
+    case kOutExrDisplay: return 16;
+    default: return 0;
+  }
+}
+
 cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, const TonemapParams& p,
-                           const float* kern, const float* curves, void* out, bool rgba8,
+                           const float* kern, const float* curves, void* out, int out_kind,
                            cudaStream_t s) {
   // Shared-memory tile of 16 x 16 (else 8 x 8) output pixels when its source
   // square fits in 48 KB; the per-tap gather otherwise (large oversample
@@ -436,26 +530,29 @@ cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, cons
       break;
     }
   }
-  if (T) {
-    dim3 grid((p.width + T - 1) / T, (p.height + T - 1) / T);
-    const size_t smem = (size_t)side * side * sizeof(float4);
-    const unsigned thr = (unsigned)(T * T);
-    if (hist_u32) {
-      if (rgba8) k_tonemap_tile<true, true><<<grid, thr, smem, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out, T, side);
-      else k_tonemap_tile<true, false><<<grid, thr, smem, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out, T, side);
-    } else {
-      if (rgba8) k_tonemap_tile<false, true><<<grid, thr, smem, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out, T, side);
-      else k_tonemap_tile<false, false><<<grid, thr, smem, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out, T, side);
-    }
-    return cudaGetLastError();
+  switch (out_kind) {
+    case kOutRgba8: tonemap_launch<kOutRgba8>(hist_u32, filtered, p, kern, curves, out, T, side, s); break;
+    case kOutRgba32f: tonemap_launch<kOutRgba32f>(hist_u32, filtered, p, kern, curves, out, T, side, s); break;
+    case kOutRgba16f: tonemap_launch<kOutRgba16f>(hist_u32, filtered, p, kern, curves, out, T, side, s); break;
+    case kOutPng16: tonemap_launch<kOutPng16>(hist_u32, filtered, p, kern, curves, out, T, side, s); break;
+    case kOutExrDisplay: tonemap_launch<kOutExrDisplay>(hist_u32, filtered, p, kern, curves, out, T, side, s); break;
+    default: return cudaErrorInvalidValue;
   }
-  dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
-  if (hist_u32) {
-    if (rgba8) k_tonemap<true, true><<<grid, 256, 0, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out);
-    else k_tonemap<true, false><<<grid, 256, 0, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out);
-  } else {
-    if (rgba8) k_tonemap<false, true><<<grid, 256, 0, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out);
-    else k_tonemap<false, false><<<grid, 256, 0, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_convert_display(const float* in, uint64_t pixels, int out_kind, void* out, int sms,
+                                   cudaStream_t s) {
+  if (pixels == 0) return cudaSuccess;
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((pixels + 255) / 256, (uint64_t)sms * 8));
+  const float4* src = (const float4*)in;
+  switch (out_kind) {
+    case kOutRgba8: k_convert_display<kOutRgba8><<<grid, 256, 0, s>>>(src, pixels, out); break;
+    case kOutRgba32f: k_convert_display<kOutRgba32f><<<grid, 256, 0, s>>>(src, pixels, out); break;
+    case kOutRgba16f: k_convert_display<kOutRgba16f><<<grid, 256, 0, s>>>(src, pixels, out); break;
+    case kOutPng16: k_convert_display<kOutPng16><<<grid, 256, 0, s>>>(src, pixels, out); break;
+    case kOutExrDisplay: k_convert_display<kOutExrDisplay><<<grid, 256, 0, s>>>(src, pixels, out); break;
+    default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
@@ -533,32 +630,44 @@ __device__ __forceinline__ uint32_t half_units(float x) {
   return (uint32_t)(fminf(fmaxf(h, 0.0f), 1.0f) * 16777216.0f);
 }
 
-// Grid-stride over 16-byte words (4 rgba8 pixels or 1 rgba32f pixel), four
-// independent loads in flight per thread; one atomic per block.
-template <bool RGBA8>
+__device__ __forceinline__ uint32_t half_bits_units(uint32_t bits) {
+  return half_units(__half2float(__ushort_as_half((unsigned short)bits)));
+}
+
+// R + G + B of the pixels in one 16-byte word: 4 rgba8 pixels, 1 rgba32f
+// pixel or 2 rgba16f pixels.
+template <int kKind>
+__device__ __forceinline__ uint64_t word_luma(const uint4 v) {
+  if (kKind == kOutRgba8) return rgb8_sum(v.x) + rgb8_sum(v.y) + rgb8_sum(v.z) + rgb8_sum(v.w);
+  if (kKind == kOutRgba32f)
+    return (uint64_t)half_units(__uint_as_float(v.x)) + half_units(__uint_as_float(v.y)) +
+           half_units(__uint_as_float(v.z));
+  return (uint64_t)half_bits_units(v.x & 0xffffu) + half_bits_units(v.x >> 16) + half_bits_units(v.y & 0xffffu) +
+         half_bits_units(v.z & 0xffffu) + half_bits_units(v.z >> 16) + half_bits_units(v.w & 0xffffu);
+}
+
+// Grid-stride over 16-byte words, four independent loads in flight per
+// thread; the pixels after the last whole word (rgba8: up to 3 as u32,
+// rgba16f: 1 as two u32) are added by block 0; one atomic per block.
+template <int kKind>
 __global__ void __launch_bounds__(256) k_luma_sum(const uint4* __restrict__ img, uint64_t words,
                                                   const uint32_t* __restrict__ tail, uint32_t n_tail,
                                                   unsigned long long* sum) {
   const uint64_t stride = (uint64_t)gridDim.x * 256;
   uint64_t acc = 0;
   uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
-  auto add = [&](const uint4 v) {
-    if (RGBA8)
-      acc += rgb8_sum(v.x) + rgb8_sum(v.y) + rgb8_sum(v.z) + rgb8_sum(v.w);
-    else
-      acc += half_units(__uint_as_float(v.x)) + half_units(__uint_as_float(v.y)) +
-             half_units(__uint_as_float(v.z));
-  };
   for (; i + 3 * stride < words; i += 4 * stride) {
     const uint4 a = __ldcs(img + i), b = __ldcs(img + i + stride), c = __ldcs(img + i + 2 * stride),
                 d = __ldcs(img + i + 3 * stride);
-    add(a);
-    add(b);
-    add(c);
-    add(d);
+    acc += word_luma<kKind>(a) + word_luma<kKind>(b) + word_luma<kKind>(c) + word_luma<kKind>(d);
   }
-  for (; i < words; i += stride) add(__ldcs(img + i));
-  if (RGBA8 && blockIdx.x == 0 && threadIdx.x < n_tail) acc += rgb8_sum(tail[threadIdx.x]);
+  for (; i < words; i += stride) acc += word_luma<kKind>(__ldcs(img + i));
+  if (blockIdx.x == 0 && threadIdx.x < n_tail) {
+    if (kKind == kOutRgba8) acc += rgb8_sum(tail[threadIdx.x]);
+    if (kKind == kOutRgba16f)
+      acc += (uint64_t)half_bits_units(tail[0] & 0xffffu) + half_bits_units(tail[0] >> 16) +
+             half_bits_units(tail[1] & 0xffffu);
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   __shared__ uint64_t warp_sums[8];
@@ -573,17 +682,20 @@ __global__ void __launch_bounds__(256) k_luma_sum(const uint4* __restrict__ img,
 }
 }  // namespace
 
-cudaError_t launch_luma_sum(const void* img, uint64_t pixels, bool rgba8, unsigned long long* sum,
+cudaError_t launch_luma_sum(const void* img, uint64_t pixels, int kind, unsigned long long* sum,
                             int sms, cudaStream_t s) {
-  const uint64_t words = rgba8 ? pixels / 4 : pixels;
-  const uint32_t n_tail = rgba8 ? (uint32_t)(pixels % 4) : 0u;
+  const uint64_t per_word = kind == kOutRgba8 ? 4 : kind == kOutRgba16f ? 2 : 1;
+  const uint64_t words = pixels / per_word;
+  const uint32_t n_tail = (uint32_t)(pixels - words * per_word);
   const uint64_t want = (words + 255) / 256;
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sms * 8));
-  const uint32_t* tail = (const uint32_t*)img + words * 4;
-  if (rgba8)
-    k_luma_sum<true><<<grid, 256, 0, s>>>((const uint4*)img, words, tail, n_tail, sum);
-  else
-    k_luma_sum<false><<<grid, 256, 0, s>>>((const uint4*)img, words, nullptr, 0, sum);
+  const uint32_t* tail = (const uint32_t*)((const uint4*)img + words);
+  switch (kind) {
+    case kOutRgba8: k_luma_sum<kOutRgba8><<<grid, 256, 0, s>>>((const uint4*)img, words, tail, n_tail, sum); break;
+    case kOutRgba32f: k_luma_sum<kOutRgba32f><<<grid, 256, 0, s>>>((const uint4*)img, words, nullptr, 0, sum); break;
+    case kOutRgba16f: k_luma_sum<kOutRgba16f><<<grid, 256, 0, s>>>((const uint4*)img, words, tail, n_tail, sum); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 }  // namespace pyr3

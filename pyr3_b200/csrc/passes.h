@@ -26,14 +26,30 @@ struct TonemapParams {
   float hsl_hue, hsl_sat, hsl_light;  // degrees, multiplier, addend
 };
 
+// Output kinds of a present (the PYR3_OUT_* values of the C-ABI):
+//   rgba8      W x H x 4 u8, the rgba8unorm display texture;
+//   rgba32f    W x H x 4 f32, the fragment value;
+//   rgba16f    W x H x 4 binary16 (nearest even), the rgba16float texture;
+//   png16      W x H x 4 u16, displayHalfToPng16 of the rgba16float value
+//              (src/gpu-readback.ts:106-115);
+//   exr display W x H x 4 f32, displayHalfToLinearExr of it
+//              (src/gpu-readback.ts:83-104): sRGB-to-linear RGB, alpha as is.
+enum OutKind { kOutRgba8 = 0, kOutRgba32f = 1, kOutRgba16f = 2, kOutPng16 = 3, kOutExrDisplay = 4 };
+// Bytes per pixel of an output kind (0 for an unknown kind).
+size_t out_bytes_per_pixel(int out_kind);
+
 cudaError_t build_kw_table(const float* knorm, float* tab, cudaStream_t s);
 size_t kw_table_floats();
 cudaError_t launch_density(const uint32_t* hist, float* filtered, const DeParams& p,
                            const float* knorm, const float* tab, cudaStream_t s);
 // curves: 5 x 256 f32 LUT on the device (read only when p.curves_active != 0).
 cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, const TonemapParams& p,
-                           const float* kern, const float* curves, void* out, bool rgba8,
+                           const float* kern, const float* curves, void* out, int out_kind,
                            cudaStream_t s);
+// An rgba32f fragment-value image (16-byte aligned) written as another
+// output kind, with the same per-pixel steps as the tonemap's store.
+cudaError_t launch_convert_display(const float* in, uint64_t pixels, int out_kind, void* out, int sms,
+                                   cudaStream_t s);
 
 // Random-splat atomic rate: `splats` deposits of 4 saturating u32 atomics
 // (the chaos kernel's scatter) into uniformly random cells of `cells`.
@@ -52,10 +68,11 @@ cudaError_t launch_linear_export(const uint32_t* hist, uint32_t width, uint32_t 
 //   rgba32f: each of R, G, B rounded to binary16 (nearest even, the
 //            rgba16float texture the reference measures), non-finite -> 0,
 //            clamped to [0, 1], in units of 2^-24 (exact: every binary16
-//            value in [0, 1] is a multiple of 2^-24).
+//            value in [0, 1] is a multiple of 2^-24);
+//   rgba16f: the same from the binary16 values themselves.
 // img must be 16-byte aligned.  The sum does not depend on the order of the
 // additions, so it is the same on every run.
-cudaError_t launch_luma_sum(const void* img, uint64_t pixels, bool rgba8, unsigned long long* sum,
+cudaError_t launch_luma_sum(const void* img, uint64_t pixels, int kind, unsigned long long* sum,
                             int sms, cudaStream_t s);
 
 }  // namespace pyr3

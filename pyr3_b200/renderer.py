@@ -31,6 +31,12 @@ DEFAULT_WALKER_JITTER = 1e-7  # src/chaos.ts:96
 DEFAULT_FLOW_SCALE = 2.0  # src/chaos.ts:139
 
 
+# present() formats: name -> (PYR3_OUT_* kind, host dtype)
+FORMATS = {"rgba8": (_lib.OUT_RGBA8, np.uint8), "f32": (_lib.OUT_RGBA32F, np.float32),
+           "f16": (_lib.OUT_RGBA16F, np.float16), "png16": (_lib.OUT_PNG16, np.uint16),
+           "exr": (_lib.OUT_EXR_DISPLAY, np.float32)}
+
+
 def _js_round(x: float) -> int:
     return int(math.floor(x + 0.5))
 
@@ -164,10 +170,13 @@ class Renderer:
                 transparent: bool = False, out: np.ndarray | None = None,
                 fmt: str = "rgba8") -> np.ndarray:
         """Density estimation + tonemap into a host RGBA image
-        (src/renderer.ts:241)."""
-        kind = _lib.OUT_RGBA8 if fmt == "rgba8" else _lib.OUT_RGBA32F
+        (src/renderer.ts:241).  fmt (FORMATS): "rgba8", "f32" (the fragment
+        value), "f16" (the rgba16float texture), "png16" and "exr" (the
+        png16 / exr exports of src/gpu-readback.ts:83-115, computed by the
+        tonemap pass)."""
+        kind, dtype = FORMATS[fmt]
         if out is None:
-            out = np.zeros((self.height, self.width, 4), np.uint8 if kind == _lib.OUT_RGBA8 else np.float32)
+            out = np.zeros((self.height, self.width, 4), dtype)
         p = self.present_opts(genome, force_de_off, transparent)
         _lib.check(_lib.lib().pyr3_present(self._h, C.byref(p), int(total_samples), _lib.ptr(out), kind))
         return out
@@ -177,7 +186,7 @@ class Renderer:
                        fmt: str = "rgba8") -> None:
         """present() into a device buffer (a pointer to W x H RGBA u8 or f32,
         e.g. a CUDA tensor's data_ptr()), queued on the renderer's stream."""
-        kind = _lib.OUT_RGBA8 if fmt == "rgba8" else _lib.OUT_RGBA32F
+        kind = FORMATS[fmt][0]
         p = self.present_opts(genome, force_de_off, transparent)
         _lib.check(_lib.lib().pyr3_present_device(self._h, C.byref(p), int(total_samples),
                                                   C.c_void_p(int(device_out)), kind))

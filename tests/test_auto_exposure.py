@@ -197,7 +197,7 @@ def _host_present(r, g, samples, brightness, fmt="rgba8"):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("fmt", ["rgba8", "f32"])
+@pytest.mark.parametrize("fmt", ["rgba8", "f32", "f16"])
 @pytest.mark.parametrize("ratio", [2.5, 0.3, 1.05, 0.0])
 def test_device_auto_exposure_matches_oracle_loop(fmt, ratio):
     """pyr3_auto_exposure (present, device luminance, fit; 8 bytes read back
@@ -206,11 +206,13 @@ def test_device_auto_exposure_matches_oracle_loop(fmt, ratio):
     estimation adds the discs of a tile with shared-memory float atomics in
     no fixed order, and the host presents take the brightness as f32 while
     the device loop derives k1 from the f64 brightness, as the reference
-    does.  So means agree to 1e-5, brightnesses to 1e-5, f32 images to 1e-5
-    and rgba8 images to one 8-bit step on fewer than 0.1 % of the bytes."""
+    does.  So means agree to 1e-5, brightnesses to 1e-5, f32 images to 1e-5,
+    f16 images to one binary16 step and rgba8 images to one 8-bit step on
+    fewer than 0.1 % of the bytes."""
     g, r, samples = _render_plain()
     base = g.tonemap["brightness"]
-    measure = OA.mean_luminance if fmt == "rgba8" else OA.mean_luminance_rgba32f
+    measure = {"rgba8": OA.mean_luminance, "f32": OA.mean_luminance_rgba32f,
+               "f16": OA.mean_luminance_half}[fmt]
     m0 = measure(_host_present(r, g, samples, base, fmt))
     target = m0 * ratio
     ref, seq = OA.fit_brightness_to_target(base, target, m0,
@@ -227,8 +229,11 @@ def test_device_auto_exposure_matches_oracle_loop(fmt, ratio):
     if fmt == "rgba8":
         diff = np.abs(dev.astype(np.int16) - host.astype(np.int16))
         assert diff.max() <= 1 and (diff > 0).mean() < 1e-3
-    else:
+    elif fmt == "f32":
         assert np.allclose(dev, host, rtol=0, atol=1e-5, equal_nan=True)
+    else:  # one binary16 step near 1
+        assert np.allclose(dev.astype(np.float32), host.astype(np.float32), rtol=0, atol=2.0 ** -10,
+                           equal_nan=True)
     if ratio in (2.5, 0.3):
         assert fit.corrected and (abs(fit.final_mean / target - 1) <= OA.AE_DEADBAND
                                   or fit.iters == OA.AE_MAX_ITERS)
