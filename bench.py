@@ -37,6 +37,7 @@ CONFIGS = {
     "motion_4k": ("iters/s (4K, 6 xforms, 8 temporal samples)", "motion_4k"),
     "batch_256": ("iters/s (256 genomes, batched)", "batch_256"),
     "denoise": ("denoiser training pixels/s (U-Net fwd+bwd+Adam)", "denoise_set"),
+    "animate": ("iters/s (30 frames 640x360, 8 sub-frames each, batched)", "animate_preview"),
     "exposure": ("auto-exposure passes/s (1080p os 2 present + 1024-edge probe)", "headline_1080p"),
 }
 
@@ -567,6 +568,105 @@ def bench_denoise(args, ws, rank, local, dist):
     }
 
 
+def bench_animate(args, ws, rank, local, dist):
+    """Animation frames (bin/pyr3-animate.ts frame loop, src/animate-render.ts
+    renderAnimationFrame): a step = 30 frames (1 s at 30 fps) of the moving
+    6-xform genome at 640x360, 50 spp, 8 box-filtered sub-frames each -- 240
+    sub-frame genomes in one AnimationBatch graph launch -- then every frame
+    presented (DE + tonemap) into a device buffer.  The step spans the
+    batch's streams and the 30 renderers' streams, so it is timed on the
+    host clock between device synchronisations."""
+    import time as _t
+
+    import torch
+
+    from pyr3_b200 import animate as A
+    from pyr3_b200 import workloads
+
+    g0, g1 = workloads.animate_preview()
+    W, H = g0.size
+    times = [k / 30 for k in range(30)]
+    ab = A.AnimationBatch(g0, g1, times, ntemporal=8, seed=7, device=local)
+    outs = [torch.empty((H, W, 4), dtype=torch.uint8, device=f"cuda:{local}") for _ in times]
+    torch.cuda.synchronize()
+
+    def step(to_host=False):
+        ab.run()
+        ab.sync()
+        for k in range(len(times)):
+            if to_host:
+                ab.present(k)
+            else:
+                ab.renderers[k].present_device(ab.centres[k], ab.samples[k], outs[k].data_ptr())
+        for r in ab.renderers:
+            r.sync()
+
+    for _ in range(args.warmup):
+        step()
+    _barrier(dist)
+    clocks = Clocks(local) if rank == 0 else None
+    graph_ms = 0.0
+    t0 = _t.perf_counter()
+    for _ in range(args.steps):
+        step()
+        graph_ms += ab.sync()[0]
+    step_s = (_t.perf_counter() - t0) / args.steps
+    clk = clocks.stop() if clocks else None
+    t0 = _t.perf_counter()
+    for _ in range(args.steps):
+        step(to_host=True)
+    e2e_s = (_t.perf_counter() - t0) / args.steps
+    # The reference's shape: one frame after another through
+    # render_motion_frame on one renderer (pyr3_iterate per sub-frame), each
+    # presented; the first pass loads modules, the second is reported.
+    from pyr3_b200 import renderer as R
+
+    r1 = R.create_renderer(W, H, 1, device=local)
+    seq_s = 0.0
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = _t.perf_counter()
+        for k, t in enumerate(times):
+            n, _ = A.render_motion_frame(r1, g0, g1, t, ntemporal=8, seed=7)
+            r1.present_device(ab.centres[k], n, outs[k].data_ptr())
+        r1.sync()
+        seq_s = _t.perf_counter() - t0
+    r1.destroy()
+    samples = sum(ab.samples)
+    t_max = _max_over_ranks(step_s * 1e3, dist, local)
+    e2e_max = _max_over_ranks(e2e_s * 1e3, dist, local)
+    seq_max = _max_over_ranks(seq_s * 1e3, dist, local)
+    n_gen = ab.n_genomes
+    ab.destroy()
+    if rank != 0:
+        return None
+    peak, peak_kind = _peaks()
+    return {
+        "metric": CONFIGS["animate"][0], "value": ws * samples / (t_max / 1e3), "unit": "iters/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (motion_4k keyframes at 640x360, pyr3_b200/workloads.py:animate_preview)",
+        "config": {"workload": "animate", "frames": len(times), "fps": 30, "canvas": [W, H],
+                   "quality_spp": g0.quality, "ntemporal": 8, "sub_frame_genomes": n_gen,
+                   "samples_per_step": samples, "frames_per_s": ws * len(times) / (t_max / 1e3),
+                   "graph_ms_per_step": graph_ms / args.steps,
+                   "timing": "host clock between synchronisations (batch + 30 renderer streams)",
+                   "l2": "30 histograms of 3.7 MB (110 MB) rewritten every step",
+                   "parallelism": f"replicas x{ws}"},
+        "e2e": {"value": ws * samples / (e2e_max / 1e3), "unit": "iters/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": W * H * 4 * len(times),
+                "note": "every frame's RGBA8 image read back to the host"},
+        "per_frame_path": {"value": ws * samples / (seq_max / 1e3), "unit": "iters/s",
+                           "frames_per_s": ws * len(times) / (seq_max / 1e3),
+                           "note": "the same frames one after another (render_motion_frame: one "
+                                   "pyr3_iterate per sub-frame, then present), host clock"},
+        "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                     "traffic": None, "note": f"chaos kernels bound by issue/latency; peak {peak_kind}"},
+        "gpu_launches": (n_gen + 2 * len(times)) * args.steps,
+        "clocks": clk,
+    }
+
+
 def bench_exposure(args, ws, rank, local, dist):
     """Render-time auto-exposure (bin/pyr3-render.ts:487-513) after the
     headline render: a step = the preview probe (1024 x 576, 16 spp, fixed
@@ -713,6 +813,8 @@ def main():
             line = bench_denoise(args, ws, rank, local, dist)
         elif args.config == "exposure":
             line = bench_exposure(args, ws, rank, local, dist)
+        elif args.config == "animate":
+            line = bench_animate(args, ws, rank, local, dist)
         else:
             line = bench_ours(args, ws, rank, local, dist)
         if line is not None:

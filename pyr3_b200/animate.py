@@ -16,7 +16,12 @@ frame:
   reset with the centre-time genome, one iterate per sub-frame at
   time + delta[i] with walkers apportioned by filter weight and seed
   (base + i * 0x9e3779b1) mod 2^32, then a single present with the total
-  sample count.
+  sample count;
+* ``AnimationBatch`` -- the frame loop of bin/pyr3-animate.ts (frame k at
+  time k / fps, each through renderAnimationFrame) for many frames at once:
+  every frame's sub-frames go into one pyr3_batch, each frame accumulating
+  into its own renderer, so a sequence of frames too small to fill the GPU
+  one by one runs as one graph launch.
 
 The keyframe blend covers keyframes of the same structure (same xform
 count and variation lists), which is what a motion-blurred frame of one
@@ -27,10 +32,12 @@ are not restated here.
 from __future__ import annotations
 
 import copy
+import ctypes as C
 import math
 
+from . import _lib
 from .genome import Genome, Xform
-from .renderer import Renderer, compute_dispatch
+from .renderer import DEFAULT_WALKER_JITTER, GpuGenome, Renderer, compute_dispatch
 
 GOLDEN = 0x9E3779B1  # per-sub-frame seed stride (src/animate-render.ts:151)
 
@@ -135,3 +142,99 @@ def render_motion_frame(renderer: Renderer, g0: Genome, g1: Genome, time: float 
         renderer.iterate(sub, (seed + i * GOLDEN) & 0xFFFFFFFF, w, iters, **iterate_kw)
         total += w
     return total * iters, counts
+
+
+def _frame_plan(g0: Genome, g1: Genome, time: float, width: int, height: int, ntemporal: int,
+                filter_kind: str, filter_width: float, filter_exp: float, seed: int):
+    """renderAnimationFrame's plan for one frame: (centre genome, iterate
+    requests [(genome, seed, walkers, iters)], total samples)."""
+    centre = interpolate_linear(g0, g1, time)
+    walkers, iters, _ = compute_dispatch(centre.quality or 16, width, height)
+    n = max(1, int(ntemporal))
+    if n == 1:
+        return centre, [(centre, seed & 0xFFFFFFFF, walkers, iters)], walkers * iters
+    deltas, filt, _ = temporal_filter(n, filter_kind, filter_width, filter_exp)
+    reqs = [(interpolate_linear(g0, g1, time + deltas[i]), (seed + i * GOLDEN) & 0xFFFFFFFF, w, iters)
+            for i, w in enumerate(apportion_walkers(walkers, filt)) if w > 0]
+    return centre, reqs, sum(r[2] for r in reqs) * iters
+
+
+class AnimationBatch:
+    """Frames at `times` of the two-keyframe animation g0 -> g1, rendered
+    together: frame k is renderAnimationFrame (src/animate-render.ts:73-176)
+    at times[k] -- its renderer reset with the centre genome, one iterate
+    per sub-frame -- and every sub-frame of every frame is one genome of a
+    single pyr3_batch, whose frames share nothing but the GPU.  run() clears
+    the frames' histograms and accumulates all of them; present(k) returns
+    frame k.  Sizes default to g0's; seed is every frame's base seed, as
+    bin/pyr3-animate.ts passes one seed to all frames.
+
+        ab = AnimationBatch(g0, g1, [k / 30 for k in range(30)], ntemporal=8)
+        ab.run(); ab.sync()
+        frames = [ab.present(k) for k in range(30)]
+    """
+
+    def __init__(self, g0: Genome, g1: Genome, times, width: int | None = None,
+                 height: int | None = None, oversample: int | None = None, ntemporal: int = 8,
+                 filter_kind: str = "box", filter_width: float = 1.0, filter_exp: float = 0.0,
+                 seed: int = 0, n_streams: int = 64, device: int = 0):
+        W = width or (g0.size[0] if g0.size else 1024)
+        H = height or (g0.size[1] if g0.size else 1024)
+        os_ = oversample or g0.oversample or 1
+        self.renderers, self.centres, self.samples = [], [], []
+        self._keep = []
+        entries = []
+        for t in times:
+            centre, reqs, total = _frame_plan(g0, g1, float(t), W, H, ntemporal, filter_kind,
+                                              filter_width, filter_exp, seed)
+            r = Renderer(W, H, os_, g0.filter_radius, device=device)
+            r.reset(centre)
+            self.renderers.append(r)
+            self.centres.append(centre)
+            self.samples.append(total)
+            entries += [(r, req) for req in reqs]
+        n = len(entries)
+        opts = (_lib.IterateOpts * n)()
+        gcs = (_lib.GenomeC * n)()
+        hs = (C.c_void_p * n)()
+        for i, (r, (g, sd, w, it)) in enumerate(entries):
+            gg = GpuGenome(g)
+            self._keep.append(gg)
+            o = opts[i]
+            o.walkers, o.iters_per_walker, o.seed = w, it, sd
+            o.walker_jitter = DEFAULT_WALKER_JITTER
+            o.flow_strength = o.trap_strength = o.phase_strength = o.phase_freq = 1.0
+            gcs[i] = gg.c
+            hs[i] = r.handle.value
+        self.n_genomes = n
+        self._opts, self._gcs, self._hs = opts, gcs, hs
+        self._b = C.c_void_p()
+        _lib.check(_lib.lib().pyr3_batch_create(hs, gcs, opts, n, n_streams, C.byref(self._b)))
+
+    def run(self) -> None:
+        """Clear every frame's histogram and accumulate all sub-frames."""
+        _lib.check(_lib.lib().pyr3_batch_run(self._b))
+
+    def sync(self):
+        """Wait for the last run; (device ms, total samples)."""
+        ms, s = C.c_float(), C.c_uint64()
+        _lib.check(_lib.lib().pyr3_batch_sync(self._b, C.byref(ms), C.byref(s)))
+        return ms.value, s.value
+
+    def present(self, k: int, **kw):
+        """Frame k: present of the centre genome with the frame's samples."""
+        return self.renderers[k].present(self.centres[k], self.samples[k], **kw)
+
+    def destroy(self) -> None:
+        if self._b:
+            _lib.lib().pyr3_batch_destroy(self._b)
+            self._b = C.c_void_p()
+        for r in self.renderers:
+            r.destroy()
+        self.renderers = []
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -92,7 +92,7 @@ def build(force: bool = False) -> str:
     cmd = [NVCC, "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
            "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared",
            "-I", os.path.join(ROOT, "include"), "-I", CSRC, *srcs, "-o", LIB,
-           "-cudart", "static", "-L", CUDA_LIB, "-lnvrtc", "-ldl",
+           "-cudart", "static", "-L", CUDA_LIB, "-lnvrtc", "-ldl", "-lpthread",
            "-Xlinker", f"-rpath,{CUDA_LIB}"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

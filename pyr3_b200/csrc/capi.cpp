@@ -824,10 +824,21 @@ struct pyr3_batch {
   std::vector<pyr3_iterate_opts> solo_o;
   std::vector<std::vector<float>> solo_xf, solo_xaos;
   std::vector<cudaEvent_t> solo_ev;
+  // Every distinct renderer of the batch, cleared once per run, and the
+  // event after those clears.
+  std::vector<pyr3_renderer*> clear_r;
+  cudaEvent_t cleared = nullptr;
+  // Pick tables of the graph genomes (one device buffer each, so genomes
+  // that share a renderer keep their own).
+  std::vector<uint16_t*> picks;
 };
 
 namespace {
 constexpr uint64_t kBatchItersPerWalker = 2000;
+// A small genome may take more walkers, down to this many iterations each
+// (the 200-iteration burn-in is then a quarter of its work), so that the
+// batch's concurrent kernels together fill the GPU.
+constexpr uint64_t kBatchMinItersPerWalker = 600;
 // Measured on the 256-genome batch: run alone, one after another, every
 // genome of 2^24 samples or more beats sharing the GPU with the graph.
 constexpr uint64_t kBatchSoloSamples = 1ull << 24;
@@ -838,6 +849,8 @@ void free_batch(pyr3_batch* b) {
   for (auto s : b->streams) cudaStreamDestroy(s);
   for (auto e : b->joins) cudaEventDestroy(e);
   for (auto e : b->solo_ev) cudaEventDestroy(e);
+  for (auto p : b->picks) cudaFree(p);
+  if (b->cleared) cudaEventDestroy(b->cleared);
   if (b->fork) cudaEventDestroy(b->fork);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
@@ -860,6 +873,7 @@ PYR3_API int pyr3_batch_create(pyr3_renderer* const* renderers, const pyr3_genom
   b->device = dev;
   CUDA_TRY(cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&b->cleared, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreate(&b->ev0));
   CUDA_TRY(cudaEventCreate(&b->ev1));
   const uint32_t k = std::min(n_streams, n);
@@ -878,6 +892,25 @@ PYR3_API int pyr3_batch_create(pyr3_renderer* const* renderers, const pyr3_genom
   std::vector<unsigned> grids;
   std::vector<pyr3_renderer*> graph_r;
   const int sms = device_sms(dev);
+  for (uint32_t i = 0; i < n; ++i)
+    if (std::find(b->clear_r.begin(), b->clear_r.end(), renderers[i]) == b->clear_r.end())
+      b->clear_r.push_back(renderers[i]);
+  // Compile every genome structure not in the cubin cache yet, in parallel
+  // on the host, before the modules load one by one below.
+  {
+    std::vector<pyr3::GenomeShape> shapes;
+    std::vector<bool> agg;
+    for (uint32_t i = 0; i < n; ++i) {
+      pyr3::GenomeShape shape;
+      if (genomes[i].xforms &&
+          pyr3::shape_from_packed(genomes[i].xforms, (int)genomes[i].n_xforms, genomes[i].final_slot, &shape)
+              .empty()) {
+        shapes.push_back(std::move(shape));
+        agg.push_back((opts[i].flags & PYR3_ITER_AGGREGATE) != 0);
+      }
+    }
+    pyr3::precompile_chaos(shapes, agg, kWpb);
+  }
   for (uint32_t i = 0; i < n; ++i) {
     pyr3_renderer* r = renderers[i];
     const pyr3_genome* g = &genomes[i];
@@ -910,16 +943,36 @@ PYR3_API int pyr3_batch_create(pyr3_renderer* const* renderers, const pyr3_genom
     int rc = pyr3::get_chaos_module(shape, kWpb, aggregate, &m, &err, inst);
     if (rc) return fail(rc, err);
     b->mods.push_back(m);
-    rc = upload_genome(r, g, *m);
-    if (rc) return rc;
-    CUDA_TRY(cudaStreamSynchronize(r->stream));
+    // This genome's own pick table; its xform records go to its module
+    // instance's constant bank.
+    {
+      const int nx = (int)g->n_xforms;
+      std::vector<float> weights(nx);
+      for (int x = 0; x < nx; ++x) weights[x] = g->xforms[(size_t)x * 116 + 3];
+      std::vector<uint16_t> starts;
+      std::string perr;
+      if (!build_pick_starts(nx, weights.data(), g->xaos, &starts, &perr)) return fail(PYR3_E_INVALID, perr);
+      uint16_t* pk = nullptr;
+      CUDA_TRY(cudaMalloc(&pk, starts.size() * 2));
+      b->picks.push_back(pk);
+      CUDA_TRY(cudaMemcpy(pk, starts.data(), starts.size() * 2, cudaMemcpyHostToDevice));
+      const size_t xf_bytes = (size_t)(nx + (g->final_slot >= 0 ? 1 : 0)) * 116 * 4;
+      if (xf_bytes > m->c_xf_bytes) return fail(PYR3_E_INVALID, "xform records exceed module constant bank");
+      CUDA_TRY(cudaMemcpy(m->c_xf, g->xforms, xf_bytes, cudaMemcpyHostToDevice));
+    }
     ChaosArgs A = base_args(r, g, o);
+    A.pick_start = b->picks.back();
     uint64_t nw;
     if (o->flags & PYR3_ITER_EXACT_WALKERS) {
       nw = std::max<uint64_t>(1, o->walkers);
     } else {
       const uint64_t cap = (uint64_t)m->blocks_per_sm * sms * m->wpb;
-      nw = std::max<uint64_t>(1, std::min<uint64_t>(cap, std::max<uint64_t>(256, total / kBatchItersPerWalker)));
+      // One kernel per stream runs at a time: each gets its share of the
+      // GPU's resident blocks, as far as its samples allow.
+      const uint64_t fill = ((uint64_t)m->blocks_per_sm * sms + k - 1) / k * m->wpb;
+      const uint64_t want = std::max<uint64_t>(std::max<uint64_t>(256, total / kBatchItersPerWalker),
+                                               std::min<uint64_t>(fill, total / kBatchMinItersPerWalker));
+      nw = std::max<uint64_t>(1, std::min<uint64_t>(cap, want));
       nw = std::min<uint64_t>(nw, std::max<uint64_t>(1, total));
     }
     A.walker_base = 0;
@@ -937,21 +990,18 @@ PYR3_API int pyr3_batch_create(pyr3_renderer* const* renderers, const pyr3_genom
     b->solo_g[s].xaos = b->solo_xaos[s].empty() ? nullptr : b->solo_xaos[s].data();
   }
   const uint32_t ng = (uint32_t)graph_r.size();
-  // Capture: fork to the worker streams, per genome clear + chaos kernel,
-  // join back.
+  // Capture: fork to the worker streams, each genome's chaos kernel, join
+  // back.  (The clears run before the graph, in pyr3_batch_run.)
   CUDA_TRY(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
   cudaError_t ce = cudaEventRecord(b->fork, b->origin);
   for (uint32_t j = 0; j < k && ce == cudaSuccess; ++j) ce = cudaStreamWaitEvent(b->streams[j], b->fork, 0);
   for (uint32_t i = 0; i < ng && ce == cudaSuccess; ++i) {
     pyr3_renderer* r = graph_r[i];
+    (void)r;
     cudaStream_t st = b->streams[i % k];
-    ce = cudaMemsetAsync(r->d_hist, 0, (size_t)r->SW * r->SH * 16, st);
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(r->d_counters, 0, 16, st);
-    if (ce == cudaSuccess) {
-      void* params[] = {&args[i]};
-      ce = cudaLaunchKernel((const void*)b->mods[i]->chaos, dim3(grids[i]), dim3(b->mods[i]->wpb), params,
-                            b->mods[i]->smem, st);
-    }
+    void* params[] = {&args[i]};
+    ce = cudaLaunchKernel((const void*)b->mods[i]->chaos, dim3(grids[i]), dim3(b->mods[i]->wpb), params,
+                          b->mods[i]->smem, st);
   }
   for (uint32_t j = 0; j < k && ce == cudaSuccess; ++j) {
     ce = cudaEventRecord(b->joins[j], b->streams[j]);
@@ -974,21 +1024,26 @@ PYR3_API int pyr3_batch_run(pyr3_batch* b) {
   if (!b) return fail(PYR3_E_INVALID, "null batch");
   cudaSetDevice(b->device);
   CUDA_TRY(cudaEventRecord(b->ev0, b->origin));
+  // Every distinct renderer once, so genomes that share one (the sub-frames
+  // of a motion-blurred frame) all accumulate into it.
+  for (pyr3_renderer* r : b->clear_r) {
+    CUDA_TRY(cudaMemsetAsync(r->d_hist, 0, (size_t)r->SW * r->SH * 16, b->origin));
+    CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, 16, b->origin));
+  }
+  CUDA_TRY(cudaEventRecord(b->cleared, b->origin));
   CUDA_TRY(cudaGraphLaunch(b->exec, b->origin));
   // Large genomes: one after another (each waits for the previous one's
   // work), beside the graph.
-  cudaEvent_t prev = b->ev0;
+  cudaEvent_t prev = b->cleared;
   for (size_t s = 0; s < b->solo_r.size(); ++s) {
     pyr3_renderer* r = b->solo_r[s];
     CUDA_TRY(cudaStreamWaitEvent(r->stream, prev, 0));
-    CUDA_TRY(cudaMemsetAsync(r->d_hist, 0, (size_t)r->SW * r->SH * 16, r->stream));
-    CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, 16, r->stream));
     const int rc = pyr3_iterate(r, &b->solo_g[s], &b->solo_o[s]);
     if (rc) return rc;
     CUDA_TRY(cudaEventRecord(b->solo_ev[s], r->stream));
     prev = b->solo_ev[s];
   }
-  if (prev != b->ev0) CUDA_TRY(cudaStreamWaitEvent(b->origin, prev, 0));
+  if (prev != b->cleared) CUDA_TRY(cudaStreamWaitEvent(b->origin, prev, 0));
   CUDA_TRY(cudaEventRecord(b->ev1, b->origin));
   return PYR3_OK;
 }

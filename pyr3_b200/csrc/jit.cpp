@@ -14,8 +14,12 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <sstream>
+#include <thread>
+#include <unordered_set>
 
 #include "pyr3.h"
 
@@ -25,6 +29,11 @@ namespace {
 
 std::mutex g_mu;
 std::map<std::string, std::weak_ptr<ChaosModule>> g_chaos_cache;
+// Cubins compiled or read by this process, by cache path: a compile on
+// another thread (precompile_chaos) lands here even where the cache
+// directory cannot be written.
+std::mutex g_cubin_mu;
+std::map<std::string, std::string> g_cubins;
 std::map<int, std::shared_ptr<EvalModule>> g_eval_cache;
 
 uint64_t fnv1a(const std::string& s) {
@@ -106,7 +115,19 @@ int compile_cubin(const std::string& src, const std::string& name, std::string* 
   char hex[32];
   std::snprintf(hex, sizeof hex, "%016llx", (unsigned long long)fnv1a(key));
   const std::string path = cache_dir() + "/" + name + "-" + hex + ".cubin";
-  if (read_file(path, cubin)) return PYR3_OK;
+  {
+    std::lock_guard<std::mutex> lk(g_cubin_mu);
+    auto it = g_cubins.find(path);
+    if (it != g_cubins.end()) {
+      *cubin = it->second;
+      return PYR3_OK;
+    }
+  }
+  if (read_file(path, cubin)) {
+    std::lock_guard<std::mutex> lk(g_cubin_mu);
+    g_cubins[path] = *cubin;
+    return PYR3_OK;
+  }
 
   nvrtcProgram prog;
   if (nvrtcCreateProgram(&prog, src.c_str(), (name + ".cu").c_str(), 0, nullptr, nullptr) !=
@@ -131,6 +152,8 @@ int compile_cubin(const std::string& src, const std::string& name, std::string* 
   nvrtcGetCUBIN(prog, &(*cubin)[0]);
   nvrtcDestroyProgram(&prog);
   write_file_atomic(path, *cubin);
+  std::lock_guard<std::mutex> lk(g_cubin_mu);
+  g_cubins[path] = *cubin;
   return PYR3_OK;
 }
 
@@ -280,6 +303,27 @@ std::string shape_from_packed(const float* xforms, int n, int final_slot, Genome
     if (!e.empty()) return "final xform: " + e;
   }
   return "";
+}
+
+void precompile_chaos(const std::vector<GenomeShape>& shapes, const std::vector<bool>& aggregate, int wpb) {
+  std::unordered_set<std::string> seen;
+  std::vector<const std::string*> srcs;
+  for (size_t i = 0; i < shapes.size(); ++i) {
+    auto ins = seen.insert(gen_chaos_source(shapes[i], wpb, aggregate[i]));
+    if (ins.second) srcs.push_back(&*ins.first);
+  }
+  if (srcs.size() < 2) return;  // nothing to overlap
+  const size_t nt = std::min<size_t>(srcs.size(), std::max(1u, std::thread::hardware_concurrency()));
+  std::atomic<size_t> next{0};
+  std::vector<std::thread> ts;
+  for (size_t t = 0; t < nt; ++t)
+    ts.emplace_back([&] {
+      for (size_t i; (i = next++) < srcs.size();) {
+        std::string cubin, err;
+        compile_cubin(*srcs[i], "chaos", &cubin, &err);  // errors surface in get_chaos_module
+      }
+    });
+  for (auto& t : ts) t.join();
 }
 
 int get_chaos_module(const GenomeShape& s, int wpb, bool aggregate,

@@ -92,6 +92,12 @@ struct EvalModule {
 // xform bank), for batches holding several genomes of one structure.
 int get_chaos_module(const GenomeShape& s, int wpb, bool aggregate,
                      std::shared_ptr<ChaosModule>* out, std::string* err, int instance = 0);
+// Compile the chaos modules of these shapes (aggregate[i] per shape) on
+// parallel host threads, one per distinct source, into the cubin cache
+// that get_chaos_module reads; compile errors are left for
+// get_chaos_module to report.  NVRTC runs on the host: a batch of many new
+// structures compiles in the time of the slowest few.
+void precompile_chaos(const std::vector<GenomeShape>& shapes, const std::vector<bool>& aggregate, int wpb);
 // Generate and compile (no device needed) the chaos module source; returns
 // the cubin size through *bytes.  Used by CPU-side build checks.
 int compile_chaos_only(const GenomeShape& s, int wpb, bool aggregate, size_t* bytes,

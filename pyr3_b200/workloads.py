@@ -145,6 +145,23 @@ def motion_4k(seed: int = 3):
     return g0, g1
 
 
+def animate_preview(seed: int = 3):
+    """The motion_4k keyframes as a preview animation: 640x360, oversample
+    1, 50 spp (DE radii kept); returns (g0, g1) at t = 0 and t = 1."""
+    import copy
+
+    out = []
+    for g in motion_4k(seed):
+        p = copy.deepcopy(g)
+        p.name = "animate-preview-6xf"
+        p.size = (640, 360)
+        p.scale = 640 / 4
+        p.oversample = 1
+        p.quality = 50
+        out.append(p)
+    return tuple(out)
+
+
 def batch_256(seed: int = 4, n: int = 256):
     rng = np.random.Generator(np.random.PCG64(seed))
     canvases = [(256, 256), (512, 512), (800, 600), (1024, 768)]

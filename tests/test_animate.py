@@ -120,3 +120,77 @@ def test_motion_frame_matches_reference_subframe_loop():
     print(f"motion log-density L1 {l1:.4%} (ref-vs-ref {floor:.4%})")
     assert l1 <= max(0.01, 1.5 * floor), (l1, floor)
     r.destroy()
+
+
+def _logd(h):
+    return np.log1p(h.reshape(-1, 4)[:, 3].astype(np.float64) / 255.0)
+
+
+@pytest.mark.gpu
+def test_animation_batch_frames_match_the_frame_loop():
+    """Six frames of the moving C1 genome, 4 box sub-frames each, rendered
+    by one AnimationBatch (24 genomes in one graph, 4 per renderer): every
+    frame accumulates exactly its sample count, and its histogram matches
+    render_motion_frame of the same frame within 1 % log-density L1 or
+    1.5x the floor between two seeds of render_motion_frame."""
+    from pyr3_b200 import renderer as R
+
+    W, H = 160, 120
+    g0, g1 = _motion_pair()
+    for g in (g0, g1):
+        g.scale = W / 4
+        g.quality = 400
+        g.size = (W, H)
+    times = [0.2, 0.3, 0.4, 0.5, 0.6, 0.7]
+    ab = A.AnimationBatch(g0, g1, times, ntemporal=4, seed=5)
+    assert ab.n_genomes == 24
+    ab.run()
+    _, total = ab.sync()
+    assert total == sum(ab.samples)
+    r = R.create_renderer(W, H, 1)
+    worst = []
+    for k, t in enumerate(times):
+        assert ab.renderers[k].counters()[0] == ab.samples[k]
+        a = _logd(ab.renderers[k].read_histogram()[0])
+        n1, _ = A.render_motion_frame(r, g0, g1, t, ntemporal=4, seed=9)
+        b = _logd(r.read_histogram()[0])
+        A.render_motion_frame(r, g0, g1, t, ntemporal=4, seed=31)
+        b2 = _logd(r.read_histogram()[0])
+        assert n1 == ab.samples[k]
+        l1 = float(np.abs(a - b).sum() / b.sum())
+        floor = float(np.abs(b2 - b).sum() / b.sum())
+        worst.append((l1, floor))
+        assert l1 <= max(0.01, 1.5 * floor), (k, l1, floor)
+    print("frame L1 vs floor:", [f"{a:.3%}/{b:.3%}" for a, b in worst])
+    img = ab.present(2)
+    assert img.shape == (H, W, 4) and img[..., :3].any()
+    # a second run clears and re-accumulates: the same counts again
+    ab.run()
+    ab.sync()
+    assert [rr.counters()[0] for rr in ab.renderers] == ab.samples
+    ab.destroy()
+    r.destroy()
+
+
+@pytest.mark.gpu
+def test_animation_batch_mixes_graph_and_solo_sub_frames_in_one_frame():
+    """A gaussian temporal filter splits walkers unevenly, so the middle
+    sub-frames of a high-quality frame reach 2^24 samples and run through
+    pyr3_iterate beside the graph while its tails run in the graph, all
+    into the same histogram: the frame still counts exactly its samples."""
+    W, H = 160, 120
+    g0, g1 = _motion_pair()
+    for g in (g0, g1):
+        g.scale = W / 4
+        g.quality = 4500
+        g.size = (W, H)
+    ab = A.AnimationBatch(g0, g1, [0.3, 0.6], ntemporal=7, filter_kind="gaussian", seed=3)
+    _, reqs, total = A._frame_plan(g0, g1, 0.3, W, H, 7, "gaussian", 1.0, 0.0, 3)
+    sizes = [w * it for _, _, w, it in reqs]
+    assert max(sizes) >= 1 << 24 and min(sizes) < 1 << 24, sizes
+    ab.run()
+    ab.sync()
+    assert [r.counters()[0] for r in ab.renderers] == ab.samples
+    hist = ab.renderers[0].read_histogram()[0]
+    assert int(hist.reshape(-1, 4)[:, 3].astype(np.uint64).sum()) == 255 * ab.renderers[0].counters()[1]
+    ab.destroy()
