@@ -11,6 +11,7 @@ C-ABI (libpyr3cuda.so).
   equal sample count.
 """
 import ctypes as C
+import math
 
 import numpy as np
 import pytest
@@ -390,6 +391,107 @@ def test_whole_render_statistical_parity(kind):
     psnr = 10 * np.log10(1.0 / max(mse, 1e-20))
     print(f"log-density L1 {l1:.4%} (ref-vs-ref {floor:.4%})  PSNR {psnr:.2f} dB")
     assert psnr >= 40.0
+    r.destroy()
+
+
+# Render-time colour modes and xform blend (chaos.wgsl:8630-8697, :8372-8381;
+# uniform slots 15-30 of src/chaos.ts:421-456): (reference uniform slots,
+# Renderer.iterate keywords, genome.xform_blend).
+_COLOUR_CASES = {
+    "flow": ({15: ("u", 1), 16: ("f", 0.8), 17: ("f", 2.0)},
+             dict(color_mode="flow", flow_strength=0.8, flow_scale=2.0), 0.0),
+    "trap_circle_rings": ({15: ("u", 2), 18: ("u", 1), 19: ("u", 1), 20: ("f", 0.1), 21: ("f", -0.2),
+                           22: ("f", 0.6), 23: ("f", -math.sin(math.radians(30.0))),
+                           24: ("f", math.cos(math.radians(30.0))), 25: ("f", 3.0), 26: ("f", 5.0),
+                           27: ("f", 0.9)},
+                          dict(color_mode="trap-distance",
+                               trap={"kind": "circle", "mode": "rings", "cx": 0.1, "cy": -0.2, "radius": 0.6,
+                                     "angle": 30.0, "falloff": 3.0, "freq": 5.0, "strength": 0.9}), 0.0),
+    "trap_line_falloff": ({15: ("u", 2), 18: ("u", 2), 19: ("u", 0), 23: ("f", -math.sin(math.radians(-40.0))),
+                           24: ("f", math.cos(math.radians(-40.0))), 22: ("f", 0.5), 25: ("f", 2.5),
+                           26: ("f", 4.0), 27: ("f", 1.0)},
+                          dict(color_mode="trap-distance",
+                               trap={"kind": "line", "angle": -40.0, "falloff": 2.5}), 0.0),
+    "phase": ({15: ("u", 3), 28: ("f", 0.7), 29: ("f", 2.0)},
+              dict(color_mode="phase", phase_strength=0.7, phase_freq=2.0), 0.0),
+    "xform_blend": ({30: ("f", 0.5)}, {}, 0.5),
+}
+
+
+def _ref_histogram_slots(g, W, H, iters, walkers, seed, slots):
+    """_ref_histogram with extra uniform slots set (slot -> ("u"|"f", value))."""
+    xf = G.pack_xforms(g)
+    pal = G.bake_lut(g.palette)
+    distrib = O.pack_xform_distrib([x.weight for x in g.xforms])
+    u = np.zeros(31, np.uint32)
+    f = u.view(np.float32)
+    i32 = u.view(np.int32)
+    u[0], u[1], u[2], u[3] = W, H, iters, 200
+    f[4], f[5], f[6] = g.scale, 0.0, 0.0
+    u[7] = seed
+    i32[8] = -1
+    u[12] = walkers
+    f[13] = 1e-7
+    f[16], f[17], f[22], f[24], f[25], f[26], f[27], f[28], f[29] = 1.0, 2.0, 0.5, 1.0, 2.0, 4.0, 1.0, 1.0, 1.0
+    for k, (t, v) in slots.items():
+        if t == "u":
+            u[k] = v
+        else:
+            f[k] = v
+    hist = np.zeros(W * H * 4, np.uint32)
+    O.ref_chaos_run(u, xf, len(g.xforms), pal, distrib, O.pack_isaac_states(walkers, seed), 0,
+                    walkers, hist, 16)
+    return hist
+
+
+@pytest.mark.parametrize("case", sorted(_COLOUR_CASES))
+@pytest.mark.parametrize("kernel", ["barrier", "wave"])
+def test_colour_modes_and_xform_blend_statistical_parity(case, kernel):
+    """Flow, trap (circle rings, line falloff) and phase colouring and the
+    xform blend on the C1 genome, 160x120, 1024 x 48k samples: the CUDA
+    renderer vs the reference's chaos_main with the same uniform slots.  The
+    count channel keeps the whole-render bar (log-density L1 <= 1 % or 1.5x
+    the reference-vs-reference floor); the colours are compared through the
+    tonemapped image, whose PSNR against the reference must be within 1 dB
+    of the reference-vs-reference PSNR at another seed, or >= 40 dB."""
+    slots, kw, blend = _COLOUR_CASES[case]
+    W, H, walkers, iters = 160, 120, 1024, 48_000
+    g = workloads.plain_small()
+    g.scale = W / 4
+    g.xform_blend = blend
+    ref = _ref_histogram_slots(g, W, H, iters, walkers, 9, slots)
+    ref2 = _ref_histogram_slots(g, W, H, iters, walkers, 31, slots)
+    samples = walkers * iters
+    r = R.create_renderer(W, H, 1)
+    r.reset(g)
+    r.iterate(g, seed=77, walkers=walkers, iters_per_walker=iters, kernel=kernel, **kw)
+    assert r.counters()[0] == samples
+    dev, _, _ = r.read_histogram()
+
+    def logd(h):
+        return np.log1p(_collapse(h.reshape(-1), W, H, 1)[..., 3] / 255.0)
+
+    a, b, b2 = logd(dev), logd(ref), logd(ref2)
+    l1 = float(np.abs(a - b).sum() / b.sum())
+    floor = float(np.abs(b2 - b).sum() / b.sum())
+    assert l1 <= max(0.01, 1.5 * floor), (l1, floor)
+    k1, k2 = O.derive_calibration(g.scale, samples, 4.0, 1)
+    kern = O.spatial_kernel(0.5, 1)
+
+    def img(h):
+        return O.visualize(W, H, 1, kern, np.float32(k1), np.float32(k2), 4.0, 1.0, 1.0, 0.01,
+                           src_u32=h).reshape(H, W, 4)[..., :3].astype(np.float64)
+
+    def psnr(x, y):
+        return 10 * np.log10(1.0 / max(float(((x - y) ** 2).mean()), 1e-20))
+
+    p_dev, p_floor = psnr(img(dev), img(ref)), psnr(img(ref2), img(ref))
+    print(f"{case}/{kernel}: L1 {l1:.3%} (floor {floor:.3%}), PSNR {p_dev:.2f} dB (ref-vs-ref {p_floor:.2f} dB)")
+    assert p_dev >= min(40.0, p_floor - 1.0), (p_dev, p_floor)
+    # the mode changed the colours: the plain palette render differs
+    if case != "xform_blend":
+        plain = _ref_histogram_slots(g, W, H, iters, walkers, 9, {})
+        assert psnr(img(plain), img(ref)) < p_floor
     r.destroy()
 
 
