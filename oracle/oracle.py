@@ -92,6 +92,8 @@ def ref():
         R.ref_dc_color.restype = C.c_int
         R.ref_chaos_run.argtypes = [_u32p, _f32p, C.c_int, _f32p, _u32p, _u32p, C.c_uint32,
                                     C.c_uint32, _u32p, C.c_int]
+        R.ref_chaos_run_capture.argtypes = [_u32p, _f32p, C.c_int, _f32p, _u32p, _u32p, C.c_uint32,
+                                            C.c_uint32, _u32p, _u32p, C.c_int]
         R.ref_density.argtypes = [C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float,
                                   C.c_float, C.c_float, _f32p, _u32p, _f32p, C.c_int]
         R.ref_visualize.argtypes = [C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float,
@@ -252,6 +254,16 @@ def ref_chaos_run(uniforms31, xforms, n_std, palette, distrib, isaac, w0, w1, hi
                         np.ascontiguousarray(xforms, np.float32), n_std,
                         np.ascontiguousarray(palette, np.float32),
                         np.ascontiguousarray(distrib, np.uint32), isaac, w0, w1, hist, threads)
+
+
+def ref_chaos_run_capture(uniforms31, xforms, n_std, palette, distrib, isaac, w0, w1, hist, idx_sum,
+                          threads):
+    """ref_chaos_run with the capture-index pass on (uniforms31[14] = 1)."""
+    ref().ref_chaos_run_capture(np.ascontiguousarray(uniforms31, np.uint32),
+                                np.ascontiguousarray(xforms, np.float32), n_std,
+                                np.ascontiguousarray(palette, np.float32),
+                                np.ascontiguousarray(distrib, np.uint32), isaac, w0, w1, hist, idx_sum,
+                                threads)
 
 
 def ref_density(hist, width, height, max_rad, min_rad, curve, k1, k2, threads=8):

@@ -126,6 +126,28 @@ REF_EXPORT void ref_chaos_run(const uint32_t *uniforms31, const float *xforms, i
   for (auto &th : pool) th.join();
 }
 
+// ref_chaos_run with the capture-index pass on (uniform slot 14 as given):
+// every splat also adds its colour index into idx_sum (superW x superH u32).
+REF_EXPORT void ref_chaos_run_capture(const uint32_t *uniforms31, const float *xforms, int n_std,
+                                      const float *palette, const uint32_t *distrib, uint32_t *isaac,
+                                      uint32_t w0, uint32_t w1, uint32_t *hist, uint32_t *idx_sum,
+                                      int threads) {
+  std::vector<uint32_t> full = expand_distrib(n_std, distrib);
+  if (threads < 1) threads = 1;
+  uint32_t total = w1 > w0 ? w1 - w0 : 0;
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t) {
+    pool.emplace_back([&, t]() {
+      std::vector<float> trace(16 * 1000, 0.0f);
+      bind_chaos(uniforms31, xforms, palette, full.data(), isaac, hist, idx_sum, trace.data());
+      chaos::u.trace_mode = 0u;
+      for (uint32_t k = (uint32_t)t; k < total; k += (uint32_t)threads)
+        chaos::U_chaos_main(vec3u(w0 + k, 0u, 0u));
+    });
+  }
+  for (auto &th : pool) th.join();
+}
+
 // density_main over rows [y0, y1) of a super-res histogram.
 REF_EXPORT void ref_density(uint32_t width, uint32_t height, float max_rad, float min_rad,
                             float curve, float k1, float k2, const float *knorm,

@@ -495,6 +495,63 @@ def test_colour_modes_and_xform_blend_statistical_parity(case, kernel):
     r.destroy()
 
 
+@pytest.mark.parametrize("kernel", ["barrier", "wave"])
+def test_capture_index_map_statistical_parity(kernel):
+    """setCaptureIndex(true) (chaos.wgsl:8137-8150, :8724-8728): every splat
+    also adds its colour index into idx_sum.  The C1 genome, 160x120, 1024 x
+    48k samples, against the reference's chaos_main with the capture pass
+    on: the index map's relative L1 within 1 % or 1.5x the reference-vs-
+    reference floor, and the mean colour index (sum of indices / sum of
+    counts) within 0.5 %; the count histogram is unchanged by the capture."""
+    W, H, walkers, iters = 160, 120, 1024, 48_000
+    g = workloads.plain_small()
+    g.scale = W / 4
+
+    def ref(seed):
+        xf = G.pack_xforms(g)
+        u = np.zeros(31, np.uint32)
+        f, i32 = u.view(np.float32), u.view(np.int32)
+        u[0], u[1], u[2], u[3] = W, H, iters, 200
+        f[4] = g.scale
+        u[7] = seed
+        i32[8] = -1
+        u[12] = walkers
+        f[13] = 1e-7
+        u[14] = 1
+        f[16], f[17], f[22], f[24], f[25], f[26], f[27], f[28], f[29] = 1.0, 2.0, 0.5, 1.0, 2.0, 4.0, 1.0, 1.0, 1.0
+        hist = np.zeros(W * H * 4, np.uint32)
+        idx = np.zeros(W * H, np.uint32)
+        O.ref_chaos_run_capture(u, xf, len(g.xforms), G.bake_lut(g.palette),
+                                O.pack_xform_distrib([x.weight for x in g.xforms]),
+                                O.pack_isaac_states(walkers, seed), 0, walkers, hist, idx, 16)
+        return hist, idx.astype(np.float64)
+
+    (h1, i1), (h2, i2) = ref(9), ref(31)
+    r = R.create_renderer(W, H, 1)
+    r.reset(g)
+    r.set_capture_index(True)
+    r.iterate(g, seed=77, walkers=walkers, iters_per_walker=iters, kernel=kernel)
+    m = r.read_index_map()  # readIndexMap (src/renderer.ts:205): {idxSum, count, width, height}
+    assert (m["width"], m["height"]) == (W, H)
+    idx = m["idxSum"].reshape(-1).astype(np.float64)
+    hist, _, _ = r.read_histogram()
+    assert np.array_equal(m["count"].reshape(-1), hist.reshape(-1, 4)[:, 3])
+    l1 = float(np.abs(idx - i1).sum() / i1.sum())
+    floor = float(np.abs(i2 - i1).sum() / i1.sum())
+    mean_dev = idx.sum() / hist.reshape(-1, 4)[:, 3].astype(np.float64).sum()
+    mean_ref = i1.sum() / h1.reshape(-1, 4)[:, 3].astype(np.float64).sum()
+    print(f"capture/{kernel}: index-map L1 {l1:.3%} (floor {floor:.3%}), mean index {mean_dev:.6f} vs {mean_ref:.6f}")
+    assert l1 <= max(0.01, 1.5 * floor), (l1, floor)
+    assert abs(mean_dev / mean_ref - 1) < 0.005
+    # capture leaves the count histogram as it is without capture
+    r2 = R.create_renderer(W, H, 1)
+    r2.reset(g)
+    r2.iterate(g, seed=77, walkers=walkers, iters_per_walker=iters, kernel=kernel)
+    assert np.array_equal(r2.read_histogram()[0], hist)
+    r.destroy()
+    r2.destroy()
+
+
 def _linear_genome(n=12, seed=3, blowup=False):
     """n xforms whose chains are affine maps only (linear variation, post
     affines, a final xform), so every kernel computes the same bits; with
