@@ -86,7 +86,9 @@ bool read_file(const std::string& path, std::string* out) {
 }
 
 void write_file_atomic(const std::string& path, const std::string& data) {
-  std::string tmp = path + ".tmp." + std::to_string(getpid());
+  // Unique per process and thread: two threads may write the same module.
+  std::string tmp = path + ".tmp." + std::to_string(getpid()) + "." +
+                    std::to_string(std::hash<std::thread::id>()(std::this_thread::get_id()));
   {
     std::ofstream f(tmp, std::ios::binary);
     if (!f) return;

@@ -194,3 +194,33 @@ def test_animation_batch_mixes_graph_and_solo_sub_frames_in_one_frame():
     hist = ab.renderers[0].read_histogram()[0]
     assert int(hist.reshape(-1, 4)[:, 3].astype(np.uint64).sum()) == 255 * ab.renderers[0].counters()[1]
     ab.destroy()
+
+
+def test_frame_plan_restates_render_animation_frame():
+    """The per-frame plan AnimationBatch submits (host logic, no GPU) is
+    renderAnimationFrame's (src/animate-render.ts:73-176): the centre genome
+    at the frame time, walkers apportioned by the temporal filter (zero-
+    weight tails dropped), every sub-frame at the centre's iterations,
+    seeds base + i * 0x9e3779b1, and a total of walkers x iterations."""
+    from pyr3_b200.renderer import compute_dispatch
+
+    g0, g1 = _motion_pair()
+    for g in (g0, g1):
+        g.quality = 50
+    W, H = 320, 180
+    for n, kind in ((1, "box"), (4, "box"), (7, "gaussian"), (9, "exp")):
+        centre, reqs, total = A._frame_plan(g0, g1, 0.4, W, H, n, kind, 1.0, 0.5, 1234)
+        walkers, iters, _ = compute_dispatch(50, W, H)
+        assert centre.xforms[0].a == A.interpolate_linear(g0, g1, 0.4).xforms[0].a
+        assert all(it == iters for _, _, _, it in reqs)
+        if n == 1:
+            assert [(s, w) for _, s, w, _ in reqs] == [(1234, walkers)]
+            continue
+        deltas, filt, _ = A.temporal_filter(n, kind, 1.0, 0.5)
+        counts = A.apportion_walkers(walkers, filt)
+        kept = [i for i, c in enumerate(counts) if c > 0]
+        assert [w for _, _, w, _ in reqs] == [counts[i] for i in kept]
+        assert [s for _, s, _, _ in reqs] == [(1234 + i * A.GOLDEN) & 0xFFFFFFFF for i in kept]
+        for (g, _, _, _), i in zip(reqs, kept):
+            assert g.xforms[1].e == A.interpolate_linear(g0, g1, 0.4 + deltas[i]).xforms[1].e
+        assert total == sum(counts) * iters == walkers * iters

@@ -152,3 +152,16 @@ def test_mean_luminance_of_the_half_texture():
         m = AE.mean_luminance(r, img)
         assert m == pytest.approx(OA.mean_luminance_half(bits.view(np.float16)), rel=1e-12, abs=1e-300), n
     r.destroy()
+
+
+def test_present_formats_map_to_the_c_abi_kinds():
+    """Renderer.present's format names, the PYR3_OUT_* kinds and their host
+    element types (host logic, no GPU)."""
+    import re
+
+    hdr = open(__import__("os").path.join(__import__("os").path.dirname(__file__), "..", "include",
+                                          "pyr3.h")).read()
+    kinds = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define PYR3_OUT_(\w+) (\d+)", hdr)}
+    assert kinds == {"RGBA8": 0, "RGBA32F": 1, "RGBA16F": 2, "PNG16": 3, "EXR_DISPLAY": 4}
+    assert {k: v[0] for k, v in R.FORMATS.items()} == {"rgba8": 0, "f32": 1, "f16": 2, "png16": 3, "exr": 4}
+    assert [np.dtype(v[1]).itemsize * 4 for v in R.FORMATS.values()] == [4, 16, 8, 8, 16]
