@@ -82,7 +82,7 @@ def test_oracle_unet_gradient_matches_torch_autograd():
     tl.backward()
     tg = np.concatenate([np.concatenate([w.grad.numpy().ravel(), b.grad.numpy().ravel()]) for w, b in layers])
     assert np.allclose(out, tout.detach().numpy(), atol=1e-10)
-    assert abs(loss / out.size - float(tl)) < 1e-12
+    assert abs(loss / out.size - float(tl.detach())) < 1e-12
     assert np.allclose(grad, tg, rtol=1e-8, atol=1e-12)
 
 
