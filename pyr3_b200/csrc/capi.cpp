@@ -477,10 +477,18 @@ int launch_chaos(pyr3_renderer* r, const pyr3::ChaosModule& m, bool queue, Chaos
 // launch fills the GPU twice over; at most 2^20, whose state (42 u32 per
 // walker and region, two buffers) stays within a few GB.
 constexpr uint64_t kWaveMaxWalkers = 1ull << 21;
+// Walkers of a wave launch: total / 2000 for large launches (2,000
+// iterations each), at least enough to fill the GPU twice over (two
+// populations) -- but a small launch takes only sqrt(1200 * total), since
+// every walker also runs the 200-iteration burn-in: measured on B200 at 2e6,
+// 9.4e6 and 3.4e7 samples, that is within 5 % of the best walker count,
+// where the fill alone was 7-38 % slower.
 uint64_t wave_walkers(pyr3_renderer* r, const pyr3::ChaosModule& m, uint64_t total) {
   const uint64_t fill =
       (uint64_t)device_sms(r->device) * (uint64_t)m.wave_blocks_per_sm * pyr3::kWaveBlock * 2;
-  const uint64_t want = std::min<uint64_t>(1ull << 20, std::max<uint64_t>(fill, total / 2000));
+  const uint64_t small = (uint64_t)std::sqrt(1200.0 * (double)total);
+  const uint64_t want =
+      std::min<uint64_t>(1ull << 20, std::max<uint64_t>(std::min<uint64_t>(fill, small), total / 2000));
   return std::max<uint64_t>(1, std::min<uint64_t>(want, total));
 }
 
