@@ -157,7 +157,7 @@ def measure_probe_luminance(genome: Genome, long_edge: int = AE_PROBE_LONG_EDGE,
         walkers, iters, samples = compute_dispatch(probe.quality, w, h)
         r.reset(probe)
         r.iterate(probe, seed, walkers, iters)
-        img = torch.empty((h, w, 4), dtype=torch.uint8, device=torch.device("cuda", r._opts.device))
+        img = torch.empty((h, w, 4), dtype=torch.uint8, device=torch.device("cuda", r.device))
         _after_torch(img)
         r.present_device(probe, samples, img.data_ptr())
         return mean_luminance(r, img)
@@ -180,7 +180,7 @@ def auto_expose(renderer: Renderer, genome: Genome, total_samples: int, target_m
         dtype = {_lib.OUT_RGBA8: torch.uint8, _lib.OUT_RGBA32F: torch.float32,
                  _lib.OUT_RGBA16F: torch.float16}[kind]
         image = torch.empty((renderer.height, renderer.width, 4), dtype=dtype,
-                            device=torch.device("cuda", renderer._opts.device))
+                            device=torch.device("cuda", renderer.device))
     elif _kind(image) != kind or image.numel() != renderer.width * renderer.height * 4:
         raise ValueError("image does not match the renderer's size and format")
     _after_torch(image)

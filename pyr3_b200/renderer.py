@@ -113,6 +113,11 @@ class Renderer:
     def handle(self):
         return self._h
 
+    @property
+    def device(self) -> int:
+        """CUDA device ordinal the renderer lives on."""
+        return self._opts.device
+
     # ---- API
     def reset(self, genome: Genome) -> None:
         """Upload the palette and zero the histogram (src/renderer.ts:221)."""
