@@ -1344,8 +1344,8 @@ PYR3_API int pyr3_mean_luminance(pyr3_renderer* r, const void* device_img, uint6
 PYR3_API int pyr3_convert_display(const void* device_rgba32f, uint64_t pixels, int32_t out_kind,
                                   void* device_out, void* stream) {
   if (pyr3::out_bytes_per_pixel(out_kind) == 0) return fail(PYR3_E_INVALID, "unknown output kind");
-  if (pixels && (!device_rgba32f || !device_out || (uintptr_t)device_rgba32f % 16 ||
-                 (uintptr_t)device_out % 16))
+  if (pixels == 0) return PYR3_OK;
+  if (!device_rgba32f || !device_out || (uintptr_t)device_rgba32f % 16 || (uintptr_t)device_out % 16)
     return fail(PYR3_E_INVALID, "convert_display: images must be 16-byte aligned device buffers");
   int dev = 0;
   CUDA_TRY(cudaGetDevice(&dev));

@@ -253,3 +253,22 @@ def test_probe_luminance_matches_host_render():
     assert target == pytest.approx(OA.mean_luminance(img), rel=1e-12)
     assert target == _exact_mean8(img)
     r.destroy()
+
+
+def test_fit_brightness_returns_the_callback_error_code():
+    """pyr3_fit_brightness (host logic): a rerender callback that fails
+    ends the fit after its first call and its code is returned, with a
+    message; a null callback is refused."""
+    calls = []
+
+    def failing(b, mean_p, ctx):
+        calls.append(b)
+        return -7
+
+    fn = _lib.RERENDER_FN(failing)
+    out = _lib.BrightnessFit()
+    rc = _lib.lib().pyr3_fit_brightness(1.0, 80.0, 10.0, fn, None, C.byref(out))
+    assert rc == -7 and calls == [8.0]
+    assert b"rerender" in _lib.lib().pyr3_last_error()
+    rc = _lib.lib().pyr3_fit_brightness(1.0, 80.0, 10.0, _lib.RERENDER_FN(0), None, C.byref(out))
+    assert rc == _lib.PYR3_E_INVALID

@@ -165,3 +165,20 @@ def test_present_formats_map_to_the_c_abi_kinds():
     assert kinds == {"RGBA8": 0, "RGBA32F": 1, "RGBA16F": 2, "PNG16": 3, "EXR_DISPLAY": 4}
     assert {k: v[0] for k, v in R.FORMATS.items()} == {"rgba8": 0, "f32": 1, "f16": 2, "png16": 3, "exr": 4}
     assert [np.dtype(v[1]).itemsize * 4 for v in R.FORMATS.values()] == [4, 16, 8, 8, 16]
+
+
+def test_convert_display_refuses_bad_arguments():
+    """pyr3_convert_display checks its kind and alignment before any device
+    work (host logic): an unknown kind and misaligned buffers are refused;
+    zero pixels is a no-op."""
+    buf = (C.c_uint8 * 64)()
+    base = C.addressof(buf)
+    aligned = base + (-base) % 16
+    L = _lib.lib()
+    assert L.pyr3_convert_display(C.c_void_p(aligned), 1, 9, C.c_void_p(aligned), None) == _lib.PYR3_E_INVALID
+    assert L.pyr3_convert_display(C.c_void_p(aligned + 4), 1, _lib.OUT_PNG16, C.c_void_p(aligned),
+                                  None) == _lib.PYR3_E_INVALID
+    assert b"aligned" in L.pyr3_last_error()
+    assert L.pyr3_convert_display(C.c_void_p(aligned), 1, _lib.OUT_PNG16, C.c_void_p(aligned + 8),
+                                  None) == _lib.PYR3_E_INVALID
+    assert L.pyr3_convert_display(None, 0, _lib.OUT_EXR_DISPLAY, None, None) == _lib.PYR3_OK
