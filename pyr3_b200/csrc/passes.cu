@@ -298,8 +298,13 @@ __device__ __forceinline__ void tonemap_pixel(float s0, float s1, float s2, floa
     const float c[3] = {s0, s1, s2};
     float nrgb[3];
     calc_newrgb(c, ls_a, p.highpow, nrgb);
+    // At vibrancy 1 the per-channel gamma term is multiplied by
+    // (1 - 1) * 256 = +0; with 0 < 1/gamma <= 1 its powf is finite for every
+    // finite sum, so the product is +0 and is not computed.
+    const bool no_perch = p.vibrancy == 1.0f && g_inv > 0.0f && g_inv <= 1.0f;
     for (int i = 0; i < 3; ++i) {
-      const float perch = (1.0f - p.vibrancy) * 256.0f * powf(fmaxf(c[i] / 255.0f, 0.0f), g_inv);
+      const float perch =
+          no_perch ? 0.0f : (1.0f - p.vibrancy) * 256.0f * powf(fmaxf(c[i] / 255.0f, 0.0f), g_inv);
       const float bg = p.transparent ? 0.0f : (1.0f - alpha) * 256.0f * p.bg[i];
       o[i] = fminf(fmaxf((nrgb[i] + perch + bg) / 256.0f, 0.0f), 1.0f);
     }
