@@ -272,3 +272,23 @@ def test_fit_brightness_returns_the_callback_error_code():
     assert b"rerender" in _lib.lib().pyr3_last_error()
     rc = _lib.lib().pyr3_fit_brightness(1.0, 80.0, 10.0, _lib.RERENDER_FN(0), None, C.byref(out))
     assert rc == _lib.PYR3_E_INVALID
+
+
+def test_probe_preset_scales_output_pixel_radii():
+    """scaleOutputPixelRadii under force mode (src/presets.test.ts:202-275):
+    DE radii and the spatial-filter radius scale with the size, the curve
+    does not; sizeScale 1 leaves them untouched; no density is safe; the
+    input genome is not changed."""
+    g = G.Genome(scale=100.0, size=(1280, 720), quality=500,
+                 density={"maxRad": 9.0, "minRad": 1.5, "curve": 0.4}, filter_radius=2.0)
+    before = copy.deepcopy(g)
+    out = AE.apply_probe_preset(g, 3840, 200)  # 3840 / 1280 = 3
+    assert out.scale == pytest.approx(300, abs=1e-6)
+    assert out.density["maxRad"] == pytest.approx(27, abs=1e-6)
+    assert out.density["minRad"] == pytest.approx(4.5, abs=1e-6) and out.density["curve"] == 0.4
+    assert out.filter_radius == pytest.approx(6, abs=1e-6)
+    assert g == before
+    same = AE.apply_probe_preset(g, 1280, 200)  # sizeScale 1
+    assert same.scale == 100 and same.density == g.density and same.filter_radius == 2.0
+    bare = AE.apply_probe_preset(G.Genome(scale=100.0, size=(1280, 720)), 3840, 200)
+    assert bare.density is None and bare.filter_radius is None
