@@ -323,9 +323,12 @@ int pyr3_density_tonemap(const uint32_t *hist, uint32_t width, uint32_t height,
  * the process exits).  Limit: width*height*oversample^2 <= 1,048,576
  * super-sampled pixels, larger canvases fail with PYR3_E_INVALID.  Runs on
  * `stream` (a cudaStream_t, NULL = default stream) of the current device.
- * The first call on a device sets the array up synchronously, so make it
- * before any stream capture.  All calls share the array: calls whose GPU
- * work overlaps race and must be serialised by the caller. */
+ * The first call on a device sets the array up, on `stream`, and waits for
+ * that set-up to finish, so make the first call before any stream capture
+ * begins.  Each call hands its filter taps and curves LUT to the device as
+ * a kernel parameter, so `p` and its curves need not outlive the call.
+ * All calls share the array: calls whose GPU work overlaps race and must
+ * be serialised by the caller. */
 int pyr3_density_tonemap_noalloc(const uint32_t *device_hist, uint32_t width, uint32_t height,
                                  uint32_t oversample, float filter_radius,
                                  const pyr3_present_opts *p, uint64_t total_samples,

@@ -101,13 +101,103 @@ def build(force: bool = False) -> str:
 
 
 CUBINS = os.path.join(PKG, "_cubins")
+SHAPES = os.path.join(PKG, "precompile_shapes.json")
 
 
 def make_cubin_cache() -> str:
     """The in-package cubin cache the library uses when PYR3_CACHE_DIR is
-    unset (filled by tests/precompile_modules.py)."""
+    unset (filled by precompile())."""
     os.makedirs(CUBINS, exist_ok=True)
     return CUBINS
+
+
+def genome_shape(g) -> dict:
+    """The structure of a genome that selects its specialised chaos module:
+    per xform the variation indices and whether it has a post affine, and
+    the same for the final xform (None without one)."""
+    from .genome import expand_for_gpu
+
+    gg = expand_for_gpu(g)
+
+    def one(x):
+        return {"vars": [int(v.index) for v in x.variations[:8]], "post": x.post is not None}
+
+    fin = gg.finalxform if (gg.finalxform is not None and gg.finalxform.active) else None
+    return {"xforms": [one(x) for x in gg.xforms], "final": one(fin) if fin is not None else None}
+
+
+def _packed_from_shape(shape):
+    """Packed xform records (the reference's 116-float layout) of a
+    structure, every numeric value a placeholder: enough to compile its
+    module, since the generated code depends only on the structure."""
+    import numpy as np
+
+    xs = shape["xforms"] + ([shape["final"]] if shape["final"] is not None else [])
+    buf = np.zeros(len(xs) * 116, np.float32)
+    for i, x in enumerate(xs):
+        o = i * 116
+        buf[o + 0], buf[o + 3], buf[o + 4 + 3], buf[o + 10] = 1.0, 1.0, len(x["vars"]), 1.0
+        buf[o + 5] = 1.0
+        if x["post"]:
+            buf[o + 12], buf[o + 15], buf[o + 17] = 1.0, 1.0, 1.0
+        for k, v in enumerate(x["vars"]):
+            buf[o + 20 + 4 * k], buf[o + 21 + 4 * k] = v, 1.0
+    return buf
+
+
+def product_genomes() -> list:
+    """Genomes of the product's own workloads whose modules the smoke run
+    and the benches load."""
+    from . import workloads
+
+    return [workloads.plain_small(), workloads.headline_1080p(), workloads.motion_4k()[0]] + \
+        workloads.denoise_set(seed=5, n=72, size=256)[:4]
+
+
+def precompile(verbose: bool = True, extra_shapes=None) -> int:
+    """NVRTC-compile (no GPU needed) every variation evaluator and the chaos
+    modules of the product workloads and of the structures listed in
+    precompile_shapes.json (those the GPU tests render), both scatter
+    variants each, into the cubin cache; returns the number of modules."""
+    import ctypes as C
+    import time
+
+    from . import _lib
+    from .renderer import GpuGenome
+
+    L = _lib.lib()
+    t = time.time()
+    bad = n = 0
+    for i in range(326):
+        impl, dc, nm = C.c_int32(), C.c_int32(), C.c_char_p()
+        L.pyr3_variation_info(i, C.byref(impl), C.byref(dc), C.byref(nm))
+        if impl.value:
+            n += 1
+            if L.pyr3_jit_compile_variation(i, C.byref(C.c_uint64())) != 0:
+                bad += 1
+    shapes = [genome_shape(g) for g in product_genomes()]
+    if os.path.exists(SHAPES):
+        shapes += json.load(open(SHAPES))["shapes"]
+    shapes += list(extra_shapes or [])
+    seen = set()
+    for sh in shapes:
+        key = json.dumps(sh, sort_keys=True)
+        if key in seen:
+            continue
+        seen.add(key)
+        buf = _packed_from_shape(sh)
+        nx = len(sh["xforms"])
+        gc = _lib.GenomeC(_lib.ptr(buf), nx, nx if sh["final"] is not None else -1, None,
+                          100.0, 0.0, 0.0, 0.0, 0, 0.0)
+        for agg in (0, 1):
+            n += 1
+            if L.pyr3_jit_compile(C.byref(gc), agg, C.byref(C.c_uint64())) != 0:
+                bad += 1
+    if bad:
+        raise RuntimeError(f"{bad} modules failed to compile: {L.pyr3_last_error().decode()[:400]}")
+    if verbose:
+        print(f"precompiled {n} modules in {time.time() - t:.0f} s")
+    return n
 
 
 if __name__ == "__main__":

@@ -1669,7 +1669,8 @@ PYR3_API int pyr3_density_tonemap_noalloc(const uint32_t* device_hist, uint32_t 
   CUDA_TRY(pyr3::noalloc_scratch(knorm, s, &sc));
   float taps[pyr3::kMaxTaps];
   const int fwidth = spatial_kernel(filter_radius > 0 ? filter_radius : 0.5f, (int)oversample, taps);
-  CUDA_TRY(cudaMemcpyAsync(sc.kern, taps, (size_t)fwidth * sizeof(float), cudaMemcpyHostToDevice, s));
+  const bool curves_on = p->curves && (p->curves_active & 31u);
+  CUDA_TRY(pyr3::noalloc_write_tables(sc, taps, fwidth, curves_on ? p->curves : nullptr, s));
   // src/calibration.ts:37-43 in double, uploaded as f32.
   const double os2 = (double)oversample * (double)oversample;
   const float k1 = (float)((p->brightness * 255.0 * 268.0) / 256.0);
@@ -1703,9 +1704,7 @@ PYR3_API int pyr3_density_tonemap_noalloc(const uint32_t* device_hist, uint32_t 
   t.bg[1] = p->background[1];
   t.bg[2] = p->background[2];
   t.transparent = p->transparent;
-  t.curves_active = p->curves ? (p->curves_active & 31u) : 0u;
-  if (t.curves_active)
-    CUDA_TRY(cudaMemcpyAsync(sc.curves, p->curves, 5 * 256 * sizeof(float), cudaMemcpyHostToDevice, s));
+  t.curves_active = curves_on ? (p->curves_active & 31u) : 0u;
   t.hsl_active = p->hsl_active ? 1u : 0u;
   t.hsl_hue = p->hsl_hue;
   t.hsl_sat = p->hsl_sat;

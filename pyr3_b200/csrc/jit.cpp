@@ -166,18 +166,26 @@ const char* cu_err(cudaError_t r) { return cudaGetErrorString(r); }
 // apply_pre_blur (chaos.wgsl:8164-8181): affine, pre_blur deltas (five
 // draws each, in slot order), variation sum in slot order with the
 // direct-colour check after each slot, post affine, colour contraction.
+// The affines, the pre_blur offset, the variation sum and the colour mix
+// round every product and sum on its own (aff_rn, mix_rn, __fadd_rn), as
+// the reference's f32 expressions do, so no FMA contraction moves their
+// last bit; pre_blur's cos / sin are the f32 roundings of the double
+// values (sincos_rn).  An affine-only genome then iterates bit for bit as
+// the reference does.
 std::string gen_chain(const XformShape& x, const std::string& base, const char* pz) {
   std::ostringstream o;
   o << "  const float* X = " << base << ";\n";
-  o << "  float2 t = f2(X[0] * p.x + X[1] * p.y + X[2], X[4] * p.x + X[5] * p.y + X[6]);\n";
+  o << "  float2 t = f2(aff_rn(X[0], p.x, X[1], p.y, X[2]), aff_rn(X[4], p.x, X[5], p.y, X[6]));\n";
   for (size_t j = 0; j < x.vars.size(); ++j) {
     if (x.vars[j] != 97) continue;
     const int wi = 21 + 4 * (int)j;
     o << "  { const float g0 = rand01(c.rng), g1 = rand01(c.rng), g2 = rand01(c.rng), "
          "g3 = rand01(c.rng);\n"
-      << "    const float g = X[" << wi << "] * (g0 + g1 + g2 + g3 - 2.0f);\n"
-      << "    const float ang = rand01(c.rng) * P_TAU;\n"
-      << "    t = f2(t.x + cosf(ang) * g, t.y + sinf(ang) * g); }\n";
+      << "    const float g = __fmul_rn(X[" << wi
+      << "], __fsub_rn(__fadd_rn(__fadd_rn(__fadd_rn(g0, g1), g2), g3), 2.0f));\n"
+      << "    const float ang = __fmul_rn(rand01(c.rng), P_TAU);\n"
+      << "    const float2 sc = sincos_rn(ang);\n"
+      << "    t = f2(__fadd_rn(t.x, __fmul_rn(sc.y, g)), __fadd_rn(t.y, __fmul_rn(sc.x, g))); }\n";
   }
   o << "  float2 acc = f2(0.0f, 0.0f);\n";
   for (size_t j = 0; j < x.vars.size(); ++j) {
@@ -189,16 +197,18 @@ std::string gen_chain(const XformShape& x, const std::string& base, const char* 
     o << "  { const float P" << j << "[10] = {X[" << b + 2 << "], X[" << b + 3 << "], X[" << e
       << "], X[" << e + 1 << "], X[" << e + 2 << "], X[" << e + 3 << "], X[" << e2 << "], X["
       << e2 + 1 << "], X[" << e2 + 2 << "], X[" << e2 + 3 << "]};\n";
-    if (pos) o << "    acc += var_" << variation_name(v) << "(t, X[" << b + 1 << "], P" << j << ", c);\n";
+    if (pos)
+      o << "    { const float2 v = var_" << variation_name(v) << "(t, X[" << b + 1 << "], P" << j
+        << ", c); acc = f2(__fadd_rn(acc.x, v.x), __fadd_rn(acc.y, v.y)); }\n";
     if (dc)
       o << "    if (X[11] > 0.5f && X[" << b + 1 << "] > 0.0f) { o.dc = dc_" << variation_name(v)
         << "(t, P" << j << "); o.dc_hit = 1; }\n";
     o << "  }\n";
   }
   if (x.has_post)
-    o << "  acc = f2(X[12] * acc.x + X[13] * acc.y + X[14], X[16] * acc.x + X[17] * acc.y + "
-         "X[18]);\n";
-  o << "  o.pv = acc;\n  o.nz = wmix(" << pz << ", X[8], X[9]);\n";
+    o << "  acc = f2(aff_rn(X[12], acc.x, X[13], acc.y, X[14]), aff_rn(X[16], acc.x, X[17], acc.y, "
+         "X[18]));\n";
+  o << "  o.pv = acc;\n  o.nz = mix_rn(" << pz << ", X[8], X[9]);\n";
   return o.str();
 }
 

@@ -172,14 +172,36 @@ VDEV void add_sat(u32* cell, u32 delta) {
   if (old > 0xffffffffu - delta) atomicOr(cell, 0xffffffffu);
 }
 
-VDEV float3 mix3(float3 a, float3 b, float t) {
-  return make_float3(wmix(a.x, b.x, t), wmix(a.y, b.y, t), wmix(a.z, b.z, t));
-}
-
 // Palette mix a*(1-t) + b*t with separately rounded products (no FMA), so
 // the fixed-point deposit is bit-identical to the reference arithmetic.
 VDEV float mix_rn(float a, float b, float t) {
   return __fadd_rn(__fmul_rn(a, __fsub_rn(1.0f, t)), __fmul_rn(b, t));
+}
+
+VDEV float3 mix3(float3 a, float3 b, float t) {
+  return make_float3(mix_rn(a.x, b.x, t), mix_rn(a.y, b.y, t), mix_rn(a.z, b.z, t));
+}
+
+// The reference's affine row a*x + b*y + c, evaluated left to right with
+// every product and sum rounded on its own.
+VDEV float aff_rn(float a, float x, float b, float y, float c) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a, x), __fmul_rn(b, y)), c);
+}
+
+// (sin a, cos a) as the f32 roundings of the double-precision values: the
+// correctly rounded f32 results except where a double result lies within
+// one double ulp of an f32 rounding boundary.  Used by pre_blur, whose
+// offsets then equal the reference's arithmetic bit for bit.
+OUTL float2 sincos_rn(float a) {
+  double s, c;
+  sincos((double)a, &s, &c);
+  return make_float2((float)s, (float)c);
+}
+
+// Scale-relative walker jitter (chaos.wgsl:8561-8565): v + (r - 0.5) * amp,
+// each operation rounded on its own.
+VDEV float jitter_rn(float v, float r, float amp) {
+  return __fadd_rn(v, __fmul_rn(__fsub_rn(r, 0.5f), amp));
 }
 
 VDEV void splat(const ChaosArgs& A, const float4* pal, float3 sp, float2 p_start, float opacity,
@@ -315,8 +337,8 @@ VDEV void run_chain(const ChaosArgs& A, const unsigned short* pst, int k, float2
       ob.dc = make_float3(0.0f, 0.0f, 0.0f);
       xform_chain((int)bi, p0, pz, cb, ob);
       float tb = rand01(rng);
-      o.pv = f2(wmix(o.pv.x, ob.pv.x, tb), wmix(o.pv.y, ob.pv.y, tb));
-      o.nz = wmix(o.nz, ob.nz, tb);
+      o.pv = f2(mix_rn(o.pv.x, ob.pv.x, tb), mix_rn(o.pv.y, ob.pv.y, tb));
+      o.nz = mix_rn(o.nz, ob.nz, tb);
     }
   }
 }
@@ -355,13 +377,13 @@ VDEV float3 accept_step(const ChaosArgs& A, const float4* pal, const Rng& rng, i
 #endif
   const float mag = fmaxf(fmaxf(fabsf(pv.x), fabsf(pv.y)), 1e-30f);
   const float amp = mag * A.jitter;
-  float jx = (rand01(rng) - 0.5f) * amp;
-  float jy = (rand01(rng) - 0.5f) * amp;
+  const float nx = jitter_rn(pv.x, rand01(rng), amp);
+  const float ny = jitter_rn(pv.y, rand01(rng), amp);
   if (past_fuse) {
     *acc_samples += 1;
     splat(A, pal, sp, p_start, c_xf[fn * 116 + 10], dc_hit, dc, acc_in);
   }
-  return make_float3(pv.x + jx, pv.y + jy, nz);
+  return make_float3(nx, ny, nz);
 }
 
 // One pass of the reference's iteration loop (chaos.wgsl:8330-8731) for a
@@ -504,8 +526,8 @@ chaos_kernel(const __grid_constant__ ChaosArgs A) {
             ob.dc = make_float3(0.0f, 0.0f, 0.0f);
             xform_chain((int)bi, p0, pz, cb, ob);
             float tb = rand01(cx.rng);
-            o.pv = f2(wmix(o.pv.x, ob.pv.x, tb), wmix(o.pv.y, ob.pv.y, tb));
-            o.nz = wmix(o.nz, ob.nz, tb);
+            o.pv = f2(mix_rn(o.pv.x, ob.pv.x, tb), mix_rn(o.pv.y, ob.pv.y, tb));
+            o.nz = mix_rn(o.nz, ob.nz, tb);
           }
         }
         rx[w] = o.pv.x; ry[w] = o.pv.y; rz[w] = o.nz;
@@ -559,9 +581,9 @@ chaos_kernel(const __grid_constant__ ChaosArgs A) {
 #endif
           const float mag = fmaxf(fmaxf(fabsf(pv.x), fabsf(pv.y)), 1e-30f);
           const float amp = mag * A.jitter;
-          float jx = (rand01(rng) - 0.5f) * amp;
-          float jy = (rand01(rng) - 0.5f) * amp;
-          wx[t] = pv.x + jx; wy[t] = pv.y + jy; wz[t] = nz;
+          const float jx = jitter_rn(pv.x, rand01(rng), amp);
+          const float jy = jitter_rn(pv.y, rand01(rng), amp);
+          wx[t] = jx; wy[t] = jy; wz[t] = nz;
           if (i >= A.fuse) {
             acc_samples += 1;
             splat(A, pal, sp, p_start, c_xf[fn * 116 + 10], dc_hit, dc, &acc_in);

@@ -65,7 +65,11 @@ cudaError_t noalloc_scratch(const float* knorm_host, cudaStream_t stream, NoAllo
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
     unsigned char* base = (unsigned char*)p;
-    e = cudaMemcpy(base + kOffKnorm, knorm_host, 257 * sizeof(float), cudaMemcpyHostToDevice);
+    // The LUT goes up on `stream`, the same stream as the table built from
+    // it, so the table never reads a half-written LUT whatever kind of
+    // stream the caller passes.
+    e = cudaMemcpyAsync(base + kOffKnorm, knorm_host, 257 * sizeof(float), cudaMemcpyHostToDevice,
+                        stream);
     if (e != cudaSuccess) return e;
     e = build_kw_table((const float*)(base + kOffKnorm), (float*)(base + kOffKw), stream);
     if (e != cudaSuccess) return e;
@@ -80,6 +84,38 @@ cudaError_t noalloc_scratch(const float* knorm_host, cudaStream_t stream, NoAllo
   out->curves = (float*)(base + kOffCurves);
   out->filtered = (float*)(base + kOffFiltered);
   return cudaSuccess;
+}
+
+namespace {
+// The per-call values, carried to the device as one kernel parameter: the
+// launch copies them, so no host buffer has to outlive the call and no copy
+// from pageable host memory is queued.
+struct NoAllocCallTables {
+  float taps[kMaxTaps];
+  float curves[5 * 256];
+  unsigned int n_taps;
+  unsigned int has_curves;
+};
+
+__global__ void k_noalloc_tables(const __grid_constant__ NoAllocCallTables t, float* kern,
+                                 float* curves) {
+  const unsigned int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < t.n_taps) kern[i] = t.taps[i];
+  if (t.has_curves && i < 5u * 256u) curves[i] = t.curves[i];
+}
+}  // namespace
+
+cudaError_t noalloc_write_tables(const NoAllocScratch& sc, const float* taps, int n_taps,
+                                 const float* curves, cudaStream_t stream) {
+  if (n_taps < 1 || n_taps > kMaxTaps) return cudaErrorInvalidValue;
+  NoAllocCallTables t;
+  for (int i = 0; i < n_taps; ++i) t.taps[i] = taps[i];
+  for (int i = n_taps; i < kMaxTaps; ++i) t.taps[i] = 0.0f;
+  t.n_taps = (unsigned int)n_taps;
+  t.has_curves = curves ? 1u : 0u;
+  for (int i = 0; i < 5 * 256; ++i) t.curves[i] = curves ? curves[i] : 0.0f;
+  k_noalloc_tables<<<5, 256, 0, stream>>>(t, sc.kern, sc.curves);
+  return cudaGetLastError();
 }
 
 }  // namespace pyr3

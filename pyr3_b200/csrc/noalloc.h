@@ -20,8 +20,14 @@ struct NoAllocScratch {
 
 // Addresses of the array on the current device.  The first call on a
 // device looks the array up with cudaGetSymbolAddress and fills the tables
-// from knorm_host (synchronously, through `stream`); later calls only
+// from knorm_host (on `stream`, then waits for it); later calls only
 // return the addresses.
 cudaError_t noalloc_scratch(const float* knorm_host, cudaStream_t stream, NoAllocScratch* out);
+
+// Write one call's spatial-filter taps (n_taps <= kMaxTaps) and, when
+// `curves` is not null, its 5 x 256 colour-curves LUT into the array, by a
+// kernel on `stream` that receives the values as its parameter.
+cudaError_t noalloc_write_tables(const NoAllocScratch& sc, const float* taps, int n_taps,
+                                 const float* curves, cudaStream_t stream);
 
 }  // namespace pyr3

@@ -18,6 +18,7 @@ import pytest
 
 from oracle import oracle as O
 from pyr3_b200 import _lib, genome as G, renderer as R, workloads
+from refrender import THREADS, TONEMAP_CASES
 
 pytestmark = pytest.mark.gpu
 
@@ -267,6 +268,74 @@ def test_density_tonemap_within_1_255(os_, de):
     else:
         src["src_u32"] = hist
     ref = O.visualize(W, H, os_, kern, np.float32(k1), np.float32(k2), 4.0, 1.0, 1.0, 0.01, **src)
+    assert float(np.abs(out - ref).max()) <= 1.0 / 255.0
+
+
+_HIST_CACHE = {}
+
+
+def _c1_histogram_cached(SW, SH):
+    """_c1_histogram of a SW x SH super-res canvas, computed once per size;
+    returns a fresh genome and the shared (read-only) histogram."""
+    if (SW, SH) not in _HIST_CACHE:
+        _HIST_CACHE[(SW, SH)] = _c1_histogram(SW, SH)
+    _, pal, hist, samples = _HIST_CACHE[(SW, SH)]
+    return workloads.plain_small(), pal, hist, samples
+
+
+@pytest.mark.parametrize("tm", TONEMAP_CASES,
+                         ids=lambda t: f"g{t[0]}-v{t[1]}-hp{t[2]}-bg{sum(t[3]) > 0:d}-tr{t[4]:d}")
+@pytest.mark.parametrize("os_,de", [(1, True), (2, True), (1, False), (2, False)])
+def test_tonemap_parameter_space_within_1_255(tm, os_, de):
+    """Density estimation + tonemap of one histogram across the tonemap's
+    parameters (gamma, vibrancy, highlight power, background, transparent
+    output; the reference's default tonemap gamma 2.4 / vibrancy 0
+    included): the device present against the oracle's density and
+    visualize within 1/255 per channel, alpha included."""
+    gamma, vib, hp, bg, transparent = tm
+    W, H = 160, 120
+    g, _, hist, samples = _c1_histogram_cached(W * os_, H * os_)
+    g.scale = W / 4
+    g.tonemap = {"gamma": gamma, "vibrancy": vib, "highlightPower": hp, "brightness": 4.0,
+                 "gammaThreshold": 0.01}
+    g.background = bg
+    p = R.Renderer.present_opts(None, g, force_de_off=not de, transparent=transparent)
+    out = np.zeros(W * H * 4, np.float32)
+    _lib.check(_lib.lib().pyr3_density_tonemap(_lib.ptr(hist), W, H, os_, 0.5, C.byref(p), samples,
+                                               _lib.ptr(out), None))
+    k1, k2 = O.derive_calibration(g.scale, samples, 4.0, os_)
+    src = {"src_u32": hist}
+    if de:
+        src = {"src_f32": O.density(hist, W * os_, H * os_, 9.0 * os_ + 1, 0.0 * os_ + 1, 0.4,
+                                    np.float32(k1), np.float32(k2))}
+    ref = O.visualize(W, H, os_, O.spatial_kernel(0.5, os_), np.float32(k1), np.float32(k2), gamma, vib, hp,
+                      0.01, bg=bg, transparent=transparent, **src)
+    err = float(np.abs(out - ref).max())
+    assert err <= 1.0 / 255.0, err
+
+
+def test_density_radius_31_within_1_255():
+    """Density estimation at the motion_4k setting, 15 / 0 / 0.6 at
+    oversample 2 (kernel radius 31, 3,969 taps per super-pixel), against
+    the oracle's density_main restatement: filtered buckets within 1e-4
+    relative at the 99.9th percentile and the tonemapped image within
+    1/255."""
+    W, H, os_ = 160, 120, 2
+    g, _, hist, samples = _c1_histogram_cached(W * os_, H * os_)
+    g.scale = W / 4
+    g.density = {"maxRad": 15.0, "minRad": 0.0, "curve": 0.6}
+    p = R.Renderer.present_opts(None, g)
+    out = np.zeros(W * H * 4, np.float32)
+    filt = np.zeros(W * os_ * H * os_ * 4, np.float32)
+    _lib.check(_lib.lib().pyr3_density_tonemap(_lib.ptr(hist), W, H, os_, 0.5, C.byref(p), samples,
+                                               _lib.ptr(out), _lib.ptr(filt)))
+    k1, k2 = O.derive_calibration(g.scale, samples, 4.0, os_)
+    ref_f = O.ref_density(hist, W * os_, H * os_, 15.0 * os_ + 1, 1.0, 0.6, np.float32(k1), np.float32(k2),
+                          threads=THREADS)
+    rel = np.abs(filt - ref_f) / np.maximum(np.abs(ref_f), 1e-3)
+    assert float(np.percentile(rel, 99.9)) < 1e-4
+    ref = O.visualize(W, H, os_, O.spatial_kernel(0.5, os_), np.float32(k1), np.float32(k2), 4.0, 1.0, 1.0,
+                      0.01, src_f32=ref_f)
     assert float(np.abs(out - ref).max()) <= 1.0 / 255.0
 
 
@@ -668,3 +737,61 @@ def test_splat_rate_deposits_every_splat():
     sums = hist.reshape(-1, 4).astype(np.uint64).sum(axis=0)
     assert ms.value > 0.0 and [int(v) for v in sums] == [1_000_003] * 4
     r.destroy()
+
+
+# ------------------------------------- bit-exact against the reference loop
+def _exact_genome():
+    """Six affine xforms (linear variation) with what the chain does besides
+    the variations: post affines, pre_blur (variation 97, five draws and a
+    cos / sin each), opacity below 1 on two xforms, a xaos matrix with a
+    zero entry, and a final xform with its own post affine behind an
+    opacity gate below 1.  Every operation is exactly rounded f32, so the
+    CUDA kernels and the reference's chaos_main compute the same bits."""
+    rng = np.random.default_rng(21)
+    lin, pre = G.variation_index("linear"), 97
+    xs = []
+    for k in range(6):
+        a, b, c, d, e, f = (float(v) for v in rng.uniform(-0.75, 0.75, 6))
+        vs = [G.Variation(lin, float(rng.uniform(0.6, 1.0)))]
+        if k in (1, 4):
+            vs.insert(0 if k == 1 else 1, G.Variation(pre, 0.04))
+        xs.append(G.Xform(a=a, b=b, c=c, d=d, e=e, f=f, weight=float(rng.uniform(0.2, 1.0)),
+                          color=float(rng.uniform(0, 1)), color_speed=float(rng.uniform(0.2, 0.8)),
+                          variations=vs, opacity=(0.55 if k == 2 else (0.3 if k == 5 else None)),
+                          xaos=[float(v) for v in rng.uniform(0.0, 2.0, 6)] if k % 2 == 0 else None,
+                          post=tuple(float(v) for v in rng.uniform(-0.9, 0.9, 6)) if k in (0, 3, 4) else None))
+    xs[2].xaos[4] = 0.0
+    fin = G.Xform(a=0.85, b=0.12, c=0.05, d=-0.1, e=0.9, f=0.02, weight=0.0, color=0.3,
+                  color_speed=0.2, variations=[G.Variation(lin, 1.0)], opacity=0.6,
+                  post=(0.95, -0.05, 0.01, 0.04, 1.02, -0.03))
+    g = workloads.plain_small()
+    g.xforms, g.finalxform = xs, fin
+    g.scale = 320 / 4
+    return g
+
+
+@pytest.mark.parametrize("kernel", ["barrier", "wave", "queue"])
+def test_kernels_equal_reference_chaos_main_bit_exact(kernel):
+    """chaos_main (chaos.wgsl:8269-8731) on the reference's own walker
+    streams: 1024 walkers seeded as packIsaacStates does, 3000 post-fuse
+    iterations each, on the genome of _exact_genome (post affines,
+    pre_blur, opacity, xaos, final xform with its opacity gate).  Each
+    CUDA chaos kernel with exact walkers gives the reference's histogram
+    bit for bit, and the same sample and in-canvas counts."""
+    from refrender import chaos as ref_chaos
+
+    g = _exact_genome()
+    W, H, walkers, iters = 320, 240, 1024, 3000
+    ref = ref_chaos(g, W, H, iters, walkers, seed=9)
+    r = R.create_renderer(W, H, 1)
+    r.reset(g)
+    r.iterate(g, seed=9, walkers=walkers, iters_per_walker=iters, exact_walkers=True, kernel=kernel)
+    s, n_in = r.counters()
+    dev, _, _ = r.read_histogram()
+    r.destroy()
+    assert s == walkers * iters
+    ref_in = int(ref.reshape(-1, 4)[:, 3].astype(np.uint64).sum())
+    diff = int((dev.reshape(-1) != ref).sum())
+    print(f"{kernel}: {n_in} in-canvas splats, {diff} differing histogram words")
+    assert n_in > walkers * iters // 4
+    assert np.array_equal(dev.reshape(-1), ref), (diff, ref_in)

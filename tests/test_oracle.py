@@ -241,3 +241,33 @@ def test_bake_curves_matches_reference_cases():
     assert lut[0] == pytest.approx(0.5, abs=1e-3) and lut[63] == pytest.approx(0.5, abs=1e-3)
     one["composite"] = [(0, 0), (0.75, 0.5)]
     assert G.bake_curves(one)[200] == pytest.approx(0.5, abs=1e-3)
+
+
+from refrender import TONEMAP_CASES  # noqa: E402
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference shaders not compiled here")
+@pytest.mark.parametrize("tm", TONEMAP_CASES, ids=lambda t: f"g{t[0]}-v{t[1]}-hp{t[2]}-bg{sum(t[3]) > 0:d}-tr{t[4]:d}")
+def test_visualize_parameter_space_restatement_matches_reference(tm):
+    """oracle.c's visualize equals the reference's WGSL on the CPU across
+    gamma, vibrancy, highlight power, background and transparency, for u32
+    (density estimation off) and f32 (density-estimated) sources at
+    oversample 1 and 2."""
+    gamma, vib, hp, bg, transparent = tm
+    rng = np.random.default_rng(7)
+    for os_ in (1, 2):
+        W, H = 24 * os_, 20 * os_
+        hist = np.zeros((H, W, 4), np.uint32)
+        cnt = rng.integers(0, 40, (H, W)) * 255
+        cnt[rng.random((H, W)) < 0.3] = 0
+        hist[..., 3] = cnt
+        for ch in range(3):
+            hist[..., ch] = (cnt * rng.random((H, W))).astype(np.uint32)
+        hist = hist.reshape(-1)
+        k1, k2 = O.derive_calibration(40, 5e4, 4, os_)
+        args = (W // os_, H // os_, os_, O.spatial_kernel(0.5, os_), k1, k2, gamma, vib, hp, 0.01)
+        kw = {"bg": bg, "transparent": transparent}
+        v1 = O.visualize(*args, src_u32=hist, **kw)
+        assert np.array_equal(v1, O.ref_visualize(*args, src_u32=hist, **kw))
+        a = O.density(hist, W, H, 9.0 * os_ + 1, 1.0, 0.4, k1, k2)
+        assert np.array_equal(O.visualize(*args, src_f32=a, **kw), O.ref_visualize(*args, src_f32=a, **kw))
