@@ -189,6 +189,19 @@ def cpu_reference_rate(g, target_seconds: float = 12.0, threads: int | None = No
     return samples / dt, threads, f"{walkers} walkers x {iters} iterations (+200 fuse) of the workload genome"
 
 
+def _config(args, g, g_close, samples, ws):
+    """The workload description both arms print (identical for the same
+    --config, so the two lines describe the same work)."""
+    W, H = g.size
+    return {"workload": args.config, "canvas": [W, H], "oversample": g.oversample,
+            "quality_spp": g.quality, "samples_per_step": samples,
+            "xforms": len(g.xforms), "final_xform": g.finalxform is not None,
+            "density_estimation": g.density is not None,
+            "temporal_samples": 8 if g_close is not None else 1,
+            "l2": "256 MiB scratch overwritten between timed steps",
+            "parallelism": f"replicas x{ws}"}
+
+
 # ------------------------------------------------------------------ ours
 def bench_ours(args, ws, rank, local, dist):
     from pyr3_b200 import _lib, renderer as R
@@ -277,22 +290,27 @@ def bench_ours(args, ws, rank, local, dist):
 
     for k in range(max(1, args.warmup // 2)):
         step_public(5000 + k)
-    e2e_ms = 0.0
+    e2e_ms, e2e_wall_ms = 0.0, 0.0
     for k in range(args.steps):
         _lib.check(lib.pyr3_flush_l2(h, L2_FLUSH))
+        r.sync()
+        t0 = time.perf_counter()
         _lib.check(lib.pyr3_mark(h, 2))
-        step_public(7000 + k)
+        step_public(7000 + k)  # ends with the blocking image read-back
         _lib.check(lib.pyr3_mark(h, 3))
+        e2e_wall_ms += (time.perf_counter() - t0) * 1e3
         ms = C.c_float()
         _lib.check(lib.pyr3_elapsed(h, 2, 3, C.byref(ms)))
         e2e_ms += ms.value
-    e2e_max = _max_over_ranks(e2e_ms, dist, local)
+    e2e_max = _max_over_ranks(e2e_wall_ms, dist, local)
+    e2e_dev_max = _max_over_ranks(e2e_ms, dist, local)
 
     if rank != 0:
         r.destroy()
         return None
     value = ws * samples * args.steps / (t_max / 1e3)
     e2e = ws * samples * args.steps / (e2e_max / 1e3)
+    e2e_dev = ws * samples * args.steps / (e2e_dev_max / 1e3)
     peak, peak_kind = _peaks()
     # Dominant kernel: the chaos kernel.  Algorithmic bytes: every in-canvas
     # splat reads and writes one 16-byte RGBA u32 bucket.  The counters
@@ -315,16 +333,14 @@ def bench_ours(args, ws, rank, local, dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded genome, pyr3_b200/workloads.py)",
-        "config": {"workload": args.config, "chaos_kernel": args.kernel, "canvas": [W, H],
-                   "oversample": os_,
-                   "quality_spp": g.quality, "samples_per_step": samples,
-                   "xforms": len(g.xforms), "final_xform": g.finalxform is not None,
-                   "density_estimation": g.density is not None,
-                   "temporal_samples": 8 if g_close is not None else 1,
-                   "l2": "256 MiB scratch overwritten between timed steps",
-                   "parallelism": f"replicas x{ws}"},
+        "config": _config(args, g, g_close, samples, ws),
+        "chaos_kernel": args.kernel,
         "e2e": {"value": e2e, "unit": "iters/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(host_img.nbytes)},
+                "d2h_bytes_per_step": int(host_img.nbytes),
+                "device_value": e2e_dev,
+                "note": "host wall clock around each public-API step (palette and genome upload, "
+                        "iterate, present, RGBA8 read back to host memory); device_value = the same "
+                        "steps timed by CUDA events on the renderer's stream"}, 
         "chaos_kernel_ms": mean_chaos,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
@@ -438,25 +454,40 @@ def _lib_flush(b):
 
 
 def bench_reference(args, ws, rank, local, dist):
+    """The reference's own chaos loop on the host cores, on the workload our
+    arm runs: each step is a bounded sample of that workload (1024 walkers,
+    fewer iterations), timed on the host clock; value = post-fuse samples
+    per second of the timed steps."""
     if rank != 0:
         return None
-    g, _ = _workload(args.config)
+    from pyr3_b200 import renderer as R
+
+    g, g_close = _workload(args.config)
+    _, _, samples = R.compute_dispatch(g.quality, *g.size)
     per = max(2.0, 60.0 / max(1, args.steps + args.warmup))
     for _ in range(args.warmup):
         cpu_reference_rate(g, target_seconds=per)
-    rates = []
+    rates, times = [], []
     sample = ""
     cores = 0
     for _ in range(args.steps):
+        t0 = time.perf_counter()
         rate, cores, sample = cpu_reference_rate(g, target_seconds=per)
+        times.append(time.perf_counter() - t0)
         rates.append(rate)
     value = statistics.mean(rates)
     return {"impl": "reference", "metric": CONFIGS[args.config][0], "value": value, "unit": "iters/s",
-            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.config},
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * statistics.mean(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded genome, pyr3_b200/workloads.py)",
+            "config": (_config(args, g, g_close, samples, ws) if args.config not in ("batch_256", "animate")
+                       else {"workload": args.config, "note": "the reference timed on the workload's "
+                                                              "first genome"}),
             "cpu_baseline": {"value": value, "unit": "iters/s", "cores": cores, "kind": "reference",
-                             "sample": sample},
+                             "sample": f"per step {sample}, extrapolated per post-fuse sample; the "
+                                       f"reference's chaos_main (src/shaders/chaos.wgsl) compiled "
+                                       f"for the CPU"},
             "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 

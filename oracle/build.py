@@ -4,7 +4,10 @@
 * oracle/_ref/libpyr3_ref.so -- the reference's own WGSL shaders
   (src/shaders/{noise_perlin,chaos,density,visualize_u32,visualize_f32}.wgsl,
   read where they lie under the reference checkout) translated to C++ by
-  oracle/wgsl2cpp.py and compiled with oracle/ref_glue.cpp.
+  oracle/wgsl2cpp.py and compiled with oracle/ref_glue.cpp;
+* oracle/_ref/libpyr3_ref64.so -- the same chaos shader with every f32
+  evaluated as a double (oracle/ref64_glue.cpp): the FP64 evaluation of the
+  variations.
 
 The reference checkout exists only in the build container; on a machine
 without it the prebuilt oracle/_ref/libpyr3_ref.so (which travels with the
@@ -73,9 +76,39 @@ def build_reference() -> str | None:
     return out
 
 
+def build_reference_f64() -> str | None:
+    """The reference's chaos shader translated with every f32 evaluated as
+    a double (oracle/_ref/libpyr3_ref64.so): the FP64 evaluation the
+    variations' f32 error is stated against.  None if the reference sources
+    are absent and no prebuilt library exists."""
+    ref_dir = os.path.join(HERE, "_ref")
+    out = os.path.join(ref_dir, "libpyr3_ref64.so")
+    if not os.path.isdir(REF_SHADERS):
+        return out if os.path.exists(out) else None
+    os.makedirs(ref_dir, exist_ok=True)
+    sys.path.insert(0, HERE)
+    import wgsl2cpp  # noqa: E402
+
+    files = ["noise_perlin.wgsl", "chaos.wgsl"]
+    deps = [os.path.join(HERE, f) for f in ("wgsl2cpp.py", "wgsl_rt.hpp", "ref64_glue.cpp")]
+    deps += [os.path.join(REF_SHADERS, f) for f in files]
+    if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+        return out
+    srcs = [open(os.path.join(REF_SHADERS, f)).read() for f in files]
+    code = wgsl2cpp.translate(srcs, "chaos64", skip_fns=("vs",), f32_type="double")
+    with open(os.path.join(ref_dir, "chaos64.cpp"), "w") as fh:
+        fh.write(code + "\n")
+    shim = os.path.join(ref_dir, "ref64_glue_tu.cpp")
+    with open(shim, "w") as fh:
+        fh.write(f'#include "{os.path.join(HERE, "ref64_glue.cpp")}"\n')
+    _run(["g++", "-std=c++17", *CFLAGS, "-I", ref_dir, shim, "-o", out])
+    return out
+
+
 def build_all() -> None:
     build_oracle()
     build_reference()
+    build_reference_f64()
 
 
 if __name__ == "__main__":

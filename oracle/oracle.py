@@ -5,7 +5,8 @@ Two libraries:
   host algorithms and of the splat / density / visualize arithmetic;
 * _ref/libpyr3_ref.so (the reference's own WGSL compiled for the CPU by
   oracle/wgsl2cpp.py): every variation, the chaos walker loop, density and
-  visualize exactly as the reference's shaders state them.
+  visualize exactly as the reference's shaders state them;
+* _ref/libpyr3_ref64.so: the same chaos shader evaluated in FP64.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this module.
@@ -103,6 +104,25 @@ def ref():
                                     C.c_float, C.c_float]
         _ref = R
     return _ref
+
+
+_ref64 = None
+
+
+def ref64():
+    """The reference's chaos shader evaluated in FP64 (oracle/_ref/libpyr3_ref64.so)."""
+    global _ref64
+    if _ref64 is None:
+        path = os.path.join(HERE, "_ref", "libpyr3_ref64.so")
+        if not os.path.exists(path):
+            from oracle import build  # noqa: PLC0415
+
+            build.build_reference_f64()
+        R = C.CDLL(path)
+        R.ref64_eval_variation_grid.argtypes = [C.c_uint32, C.c_int, _f32p, C.c_float, _f32p, _f32p,
+                                                _f32p, _u32p, _f64p]
+        _ref64 = R
+    return _ref64
 
 
 # ----------------------------------------------------------------- helpers
@@ -239,6 +259,18 @@ def ref_eval_grid(idx, pts, w, params10, a0, a1, isaac):
                                   np.ascontiguousarray(params10, np.float32),
                                   np.ascontiguousarray(a0, np.float32),
                                   np.ascontiguousarray(a1, np.float32), isaac, out)
+    return out.reshape(-1, 2)
+
+
+def ref64_eval_grid(idx, pts, w, params10, a0, a1, isaac):
+    """apply_variation of the reference's shader evaluated in FP64 (f32
+    inputs, double outputs), isaac advanced in place."""
+    pts = np.ascontiguousarray(pts, np.float32).reshape(-1)
+    out = np.zeros(len(pts), np.float64)
+    ref64().ref64_eval_variation_grid(idx, len(pts) // 2, pts, w,
+                                      np.ascontiguousarray(params10, np.float32),
+                                      np.ascontiguousarray(a0, np.float32),
+                                      np.ascontiguousarray(a1, np.float32), isaac, out)
     return out.reshape(-1, 2)
 
 

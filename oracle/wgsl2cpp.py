@@ -1163,10 +1163,18 @@ class Emitter:
         return "\n".join(o)
 
 
-def translate(sources, ns, skip_fns=()):
+def translate(sources, ns, skip_fns=(), f32_type="float"):
+    """C++ for the WGSL `sources` in namespace `ns`.  f32_type="double"
+    emits every f32 value, literal and conversion as a C++ double: the same
+    expressions evaluated in FP64, for measuring the f32 shaders' error."""
     text = "\n".join(sources)
     items = Parser(tokenize(text)).parse_module()
-    return Emitter(ns, skip_fns).translate(items)
+    saved = CPP_SCALAR["f32"]
+    CPP_SCALAR["f32"] = f32_type
+    try:
+        return Emitter(ns, skip_fns).translate(items)
+    finally:
+        CPP_SCALAR["f32"] = saved
 
 
 if __name__ == "__main__":

@@ -111,10 +111,18 @@ template <class R, class A> inline R conv(const A &a) {
   }
 }
 template <class To, class From> inline To bitcast(const From &f) {
-  static_assert(sizeof(To) == sizeof(From), "bitcast size");
-  To t;
-  std::memcpy(&t, &f, sizeof t);
-  return t;
+  if constexpr (sizeof(To) != sizeof(From) && std::is_same_v<From, double>) {
+    // FP64 build of the shaders (oracle/build.py, f32 emitted as double):
+    // a WGSL bitcast of an f32 reads the bits of the value rounded to f32.
+    return bitcast<To>((float)f);
+  } else if constexpr (sizeof(To) != sizeof(From) && std::is_same_v<To, double>) {
+    return (double)bitcast<float>(f);
+  } else {
+    static_assert(sizeof(To) == sizeof(From), "bitcast size");
+    To t;
+    std::memcpy(&t, &f, sizeof t);
+    return t;
+  }
 }
 
 // ---- elementwise helpers ----

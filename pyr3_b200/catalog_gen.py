@@ -121,7 +121,9 @@ def generate(ref_root: str) -> dict:
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PYR3_REFERENCE")
+    if not root:
+        sys.exit("usage: python -m pyr3_b200.catalog_gen REFERENCE_ROOT (or set PYR3_REFERENCE)")
     cat = generate(root)
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "catalog.json")
     with open(path, "w") as f:

@@ -1,8 +1,8 @@
 """Seeded synthetic workloads (the benchmark configurations).
 
 Every genome here is generated from a fixed seed with numpy's PCG64 so the
-same file can be rendered by the reference (`.pyr3.json`, written by
-`python -m pyr3_b200.workloads`).  Parameter draws follow the
+same file can be rendered by the reference (`.pyr3.json` in
+pyr3_b200/genomes/, written by `python -m pyr3_b200.workloads`).  Parameter draws follow the
 configuration text:
 
 * `plain_small()`  -- 640x480 os1 q50, 3 xforms (a..f ~ U[-1,1], weight
@@ -211,18 +211,33 @@ def denoise_set(seed: int = 5, n: int = 72, size: int = 256, structures: int = 4
     return out
 
 
-def write_all(outdir: str | None = None) -> None:
-    outdir = outdir or os.path.join(HERE, "workloads")
+def write_all(outdir: str | None = None) -> list:
+    """Write the benchmark genomes as `.pyr3.json` files (the reference's v1
+    schema), so the reference can render the identical genomes: the four
+    single-genome configurations (motion_4k and animate_preview as their
+    two keyframes) and the eight batch_256 genomes the parity tests render
+    (the generator reproduces the other 248 from the same seed)."""
+    outdir = outdir or os.path.join(HERE, "genomes")
     os.makedirs(outdir, exist_ok=True)
     items = {"plain_small.pyr3.json": plain_small(), "headline_1080p.pyr3.json": headline_1080p()}
     g0, g1 = motion_4k()
     items["motion_4k_open.pyr3.json"] = g0
     items["motion_4k_close.pyr3.json"] = g1
+    a0, a1 = animate_preview()
+    items["animate_preview_open.pyr3.json"] = a0
+    items["animate_preview_close.pyr3.json"] = a1
+    for g in batch_256()[:8]:
+        items[f"{g.name}.pyr3.json"] = g
+    paths = []
     for name, g in items.items():
-        with open(os.path.join(outdir, name), "w") as f:
+        path = os.path.join(outdir, name)
+        with open(path, "w") as f:
             json.dump(genome_to_json(g), f, indent=1)
             f.write("\n")
+        paths.append(path)
+    return paths
 
 
 if __name__ == "__main__":
-    write_all()
+    for p in write_all():
+        print(p)

@@ -110,4 +110,7 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PYR3_REFERENCE")
+    if not root:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT (or set PYR3_REFERENCE)")
+    main(root)

@@ -123,3 +123,18 @@ def test_variation_evaluators_compile():
         n = C.c_uint64()
         rc = _lib.lib().pyr3_jit_compile_variation(i, C.byref(n))
         assert rc == 0, _lib.lib().pyr3_last_error()
+
+
+def test_committed_genome_files_match_the_generator(tmp_path):
+    """pyr3_b200/genomes/*.pyr3.json (the benchmark genomes in the
+    reference's file format, so the reference can render them) are what
+    the seeded generator writes today."""
+    import os
+
+    from pyr3_b200 import workloads
+
+    here = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "pyr3_b200", "genomes")
+    fresh = workloads.write_all(str(tmp_path))
+    assert sorted(os.listdir(here)) == sorted(os.path.basename(p) for p in fresh)
+    for p in fresh:
+        assert open(p).read() == open(os.path.join(here, os.path.basename(p))).read(), p

@@ -142,26 +142,123 @@ def _relerr(a, b):
     return d
 
 
-@pytest.mark.parametrize("case", _impl_ids(), ids=lambda c: c[1])
-def test_variation_matches_reference(case):
-    """CUDA variation vs the reference's WGSL (f32, CPU) on a seeded grid:
-    relative error (scale max(|a|,|b|,1)) <= 1e-3 on at least 99% of points
-    and the RNG streams consume identically (same ISAAC state afterwards)."""
-    idx, name, _ = case
+def _scaled_ulps(a, b):
+    """|a - b| in units of one f32 ulp at max(|a|, |b|, 1) (2^-23 relative
+    above 1, 2^-23 absolute below): per point, the larger of x and y.
+    Equal NaNs and equal infinities count 0, a NaN against a number inf."""
+    a64, b64 = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    scale = np.maximum(np.maximum(np.abs(a64), np.abs(b64)), 1.0)
+    with np.errstate(invalid="ignore", over="ignore"):
+        d = np.abs(a64 - b64) / scale / 2.0 ** -23
+    same = (np.isnan(a64) & np.isnan(b64)) | (np.isinf(a64) & np.isinf(b64) & (np.sign(a64) == np.sign(b64)))
+    d[same] = 0.0
+    d[np.isnan(d)] = np.inf
+    return d.max(axis=1)
+
+
+def _variation_case(idx):
     rng = np.random.default_rng(idx + 11)
     pts = _grid(512, rng)
     p = _params(idx, rng)
     a0 = np.array([0.8, -0.4, 0.1, 1.0], np.float32)
     a1 = np.array([0.3, 0.5, 0.2, 1.0], np.float32)
-    isaac = O.pack_isaac_states(len(pts), 1000 + idx)
+    return pts, p, a0, a1, O.pack_isaac_states(len(pts), 1000 + idx)
+
+
+@pytest.mark.parametrize("case", _impl_ids(), ids=lambda c: c[1])
+def test_variation_matches_reference(case):
+    """CUDA variation vs the reference's WGSL (f32, CPU) and vs the same
+    WGSL evaluated in FP64, on a seeded 512-point grid:
+
+    * relative error (scale max(|a|, |b|, 1)) against the f32 reference
+      <= 1e-3 on at least 99 % of points;
+    * the RNG streams consume identically (same ISAAC state afterwards);
+    * a line of statistics: the f32 ulps (at max(|a|, |b|, 1)) against the
+      f32 reference, max and 99th percentile, and both implementations'
+      error against the FP64 evaluation."""
+    idx, name, _ = case
+    pts, p, a0, a1, isaac = _variation_case(idx)
     dev, st_dev = _eval_dev(idx, pts, 0.75, p, a0, a1, isaac)
     st_ref = isaac.copy()
     ref = O.ref_eval_grid(idx, pts, 0.75, p, a0, a1, st_ref)
+    ref64 = O.ref64_eval_grid(idx, pts, 0.75, p, a0, a1, isaac.copy())
     err = np.maximum(_relerr(dev[:, 0], ref[:, 0]), _relerr(dev[:, 1], ref[:, 1]))
     frac_ok = float((err <= 1e-3).mean())
+    same_draws = float((st_dev.reshape(-1, 36)[:, 0] == st_ref.reshape(-1, 36)[:, 0]).mean())
+    u32 = _scaled_ulps(dev, ref)
+    u_dev64, u_ref64 = _scaled_ulps(dev, ref64), _scaled_ulps(ref, ref64)
+    print(f"VARSTAT {name} ulp_vs_ref32 p99 {np.percentile(u32, 99):.4g} max {u32.max():.4g} | "
+          f"vs_fp64 dev p99 {np.percentile(u_dev64, 99):.4g} max {u_dev64.max():.4g} "
+          f"ref p99 {np.percentile(u_ref64, 99):.4g} max {u_ref64.max():.4g} | same_draws {same_draws:.4f}")
     assert frac_ok >= 0.99, (name, frac_ok, float(np.nanmax(err)))
-    same_draws = (st_dev.reshape(-1, 36)[:, 0] == st_ref.reshape(-1, 36)[:, 0]).mean()
     assert same_draws >= 0.99, (name, same_draws)
+
+
+# Variations whose trig takes coordinate- or radius-scaled arguments through
+# safe_sin / safe_cos / safe_tanh (chaos.wgsl:356-385): the reference's
+# src/chaos-safetrig.gpu.test.ts names waves, tancos, funnel, tractrix,
+# clifford_js, murl2, phoenix_julia and e_julia; sinusoidal, sin, cos, swirl
+# and disc take the same helpers.
+SAFE_TRIG_VARIATIONS = ["sinusoidal", "sin", "cos", "waves", "swirl", "disc", "tancos", "funnel",
+                        "tractrix", "clifford_js", "murl2", "phoenix_julia", "e_julia"]
+
+
+def _far_grid(n, rng):
+    """Points with |x|, |y| log-uniform in [1e6, 1e9] (random signs), where
+    safe_sin / safe_cos switch to the hash of the argument's bits, plus the
+    reference test's own points (1e10, 0.5) and (1e8, 1e8)."""
+    mag = 10.0 ** rng.uniform(6.0, 9.0, (n, 2))
+    pts = (mag * rng.choice([-1.0, 1.0], (n, 2))).astype(np.float32)
+    pts[0] = [1e10, 0.5]
+    pts[1] = [1e8, 1e8]
+    return pts
+
+
+@pytest.mark.parametrize("name", SAFE_TRIG_VARIATIONS)
+def test_safe_trig_hash_path_on_device(name):
+    """The variations above at coordinates of 1e6-1e10 on the device, where
+    native f32 trig would cliff (src/chaos-safetrig.gpu.test.ts): wherever
+    the reference's output is finite the device's is finite too, and where
+    the reference's is non-zero the device's is non-zero (no trig cliff to
+    0); a line of agreement statistics."""
+    idx = G.variation_index(name)
+    rng = np.random.default_rng(idx + 7)
+    pts = _far_grid(256, rng)
+    p = _params(idx, rng)
+    a0 = np.array([0.8, -0.4, 0.1, 1.0], np.float32)
+    a1 = np.array([0.3, 0.5, 0.2, 1.0], np.float32)
+    isaac = O.pack_isaac_states(len(pts), 77 + idx)
+    dev, _ = _eval_dev(idx, pts, 0.75, p, a0, a1, isaac)
+    ref = O.ref_eval_grid(idx, pts, 0.75, p, a0, a1, isaac.copy())
+    fin = np.isfinite(ref)
+    assert np.isfinite(dev[fin]).all(), name
+    nz = fin & (ref != 0.0)
+    assert (dev[nz] != 0.0).all(), name
+    err = np.maximum(_relerr(dev[:, 0], ref[:, 0]), _relerr(dev[:, 1], ref[:, 1]))
+    print(f"FARSTAT {name} within_1e-3 {float((err <= 1e-3).mean()):.3f} finite {float(fin.mean()):.3f}")
+
+
+def test_safe_sin_cos_at_the_cliff_on_device():
+    """src/chaos-safetrig.gpu.test.ts on the device, through var_sin and
+    var_cos at (x, 0), which return (safe_sin(x), 0) and (safe_cos(x), 0):
+    at x = 1e10 both are bounded, non-zero and on the unit circle (to 1e-4)
+    and within two f32 ulps of the reference's values (CUDA's sinf / cosf
+    against the correctly rounded f32 values); at x = 0.5 they are the
+    ordinary sin and cos, within two ulps as well."""
+    isaac = O.pack_isaac_states(2, 5)
+    pts = np.array([[1e10, 0.0], [0.5, 0.0]], np.float32)
+    p = np.zeros(10, np.float32)
+    a0 = np.array([1.0, 0.0, 0.0, 1.0], np.float32)
+    a1 = np.array([0.0, 1.0, 0.0, 1.0], np.float32)
+    s, _ = _eval_dev(G.variation_index("sin"), pts, 1.0, p, a0, a1, isaac)
+    c, _ = _eval_dev(G.variation_index("cos"), pts, 1.0, p, a0, a1, isaac)
+    rs = O.ref_eval_grid(G.variation_index("sin"), pts, 1.0, p, a0, a1, isaac.copy())
+    rc = O.ref_eval_grid(G.variation_index("cos"), pts, 1.0, p, a0, a1, isaac.copy())
+    sb, cb = float(s[0, 0]), float(c[0, 0])
+    assert 0.0 < abs(sb) <= 1.0 and 0.0 < abs(cb) <= 1.0
+    assert abs(sb * sb + cb * cb - 1.0) < 1e-4
+    assert _scaled_ulps(np.array([[sb, cb]]), np.array([[rs[0, 0], rc[0, 0]]]))[0] <= 2.0
+    assert _scaled_ulps(np.array([[s[1, 0], c[1, 0]]]), np.array([[rs[1, 0], rc[1, 0]]]))[0] <= 2.0
 
 
 def test_variations_match_flam3_goldens():

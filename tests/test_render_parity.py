@@ -67,34 +67,50 @@ def _check(name, g, dev_hist, dev_img, ref1, ref2, W, H, os_, samples):
     return l1, floor, p_dev, p_floor
 
 
-@pytest.mark.parametrize("pool", ["bench_2000_iters", "short_trajectories"])
-def test_headline_genome_matches_reference(pool):
+@pytest.mark.parametrize("pool,W,H,spp", [("bench_2000_iters", 480, 270, 500),
+                                          ("short_trajectories", 480, 270, 500),
+                                          ("bench_2000_iters", 192, 108, 6000)])
+def test_headline_genome_matches_reference(pool, W, H, spp):
     """The headline genome (1920x1080 os 2, 500 spp, 12 catalog xforms +
-    final) on a 480x270 os-2 canvas at 500 spp (6.48e7 samples) through the
-    wave kernel: with 32,400 walkers of 2,000 iterations (the bench's
-    iterations per walker: 518,400 x 2,000 at full size), and with the
-    small-launch pool (~279k walkers of ~232 iterations, where the 200-
-    iteration burn-in weighs most), against the reference's 1024 walkers
-    of 63,282 iterations (computeDispatch)."""
+    final) on reduced os-2 canvases through the wave kernel, against the
+    reference's computeDispatch split (1024 walkers):
+
+    * 480x270 at the bench's 500 spp (6.48e7 samples), with walkers of 2,000
+      iterations (the bench's iterations per walker: 518,400 x 2,000 at full
+      size), and with the small-launch pool (~279k walkers of ~232
+      iterations, where the 200-iteration burn-in weighs most).  At 500 spp
+      two reference seeds are themselves only ~32.6 dB apart, so the image
+      bar is the reference-vs-reference PSNR less 1 dB;
+    * 192x108 at 6,000 spp (1.24e8 samples), where the reference-vs-
+      reference floor is above 40 dB: the device render is at least 40 dB
+      from the reference.
+
+    With 2,000-iteration walkers the device draws samples // 2000 x 2000
+    samples (at most 1,999 fewer than the reference), and each image is
+    presented with its own sample count."""
     g = workloads.headline_1080p()
-    W, H, os_ = 480, 270, 2
+    os_ = 2
     g.scale = W / 4
-    walkers, iters, samples = R.compute_dispatch(500, W, H)
+    walkers, iters, samples = R.compute_dispatch(spp, W, H)
     ref1 = ref_chaos(g, W * os_, H * os_, iters, walkers, seed=9, oversample=os_)
     ref2 = ref_chaos(g, W * os_, H * os_, iters, walkers, seed=31, oversample=os_)
     r = R.create_renderer(W, H, os_)
     r.reset(g)
     if pool == "bench_2000_iters":
-        assert samples % 2000 == 0
-        r.iterate(g, seed=77, walkers=samples // 2000, iters_per_walker=2000, exact_walkers=True,
+        dev_samples = samples // 2000 * 2000
+        r.iterate(g, seed=77, walkers=dev_samples // 2000, iters_per_walker=2000, exact_walkers=True,
                   kernel="wave")
     else:
+        dev_samples = samples
         r.iterate(g, seed=77, walkers=walkers, iters_per_walker=iters, kernel="wave")
-    assert r.counters()[0] == samples
+    assert r.counters()[0] == dev_samples
     dev, _, _ = r.read_histogram()
-    img = r.present(g, samples, fmt="f32")[..., :3].astype(np.float64)
+    img = r.present(g, dev_samples, fmt="f32")[..., :3].astype(np.float64)
     r.destroy()
-    _check(f"headline/{pool}", g, dev.reshape(-1), img, ref1, ref2, W, H, os_, samples)
+    _, _, p_dev, p_floor = _check(f"headline/{pool}/{W}x{H}/{spp}spp", g, dev.reshape(-1), img, ref1, ref2,
+                                  W, H, os_, samples)
+    if spp >= 6000:
+        assert p_floor >= 40.0 and p_dev >= 40.0, (p_dev, p_floor)
 
 
 def test_motion_4k_genome_matches_reference_subframe_loop():
