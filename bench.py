@@ -250,7 +250,7 @@ def bench_ours(args, ws, rank, local, dist):
     r.sync()
     _barrier(dist)
     clocks = Clocks(local) if rank == 0 else None
-    total_ms, chaos_ms = 0.0, []
+    total_ms, chaos_ms, present_ms = 0.0, [], []
     launches0 = r.launches
     for k in range(args.steps):
         _lib.check(lib.pyr3_flush_l2(h, L2_FLUSH))
@@ -262,6 +262,8 @@ def bench_ours(args, ws, rank, local, dist):
         total_ms += ms.value
         _lib.check(lib.pyr3_elapsed(h, 4, 5, C.byref(ms)))
         chaos_ms.append(ms.value)
+        _lib.check(lib.pyr3_elapsed(h, 5, 1, C.byref(ms)))
+        present_ms.append(ms.value)
     clk = clocks.stop() if clocks else None
     chaos_launches = r.launches - launches0
     n_samples, n_splats = r.counters()
@@ -353,6 +355,7 @@ def bench_ours(args, ws, rank, local, dist):
             "frac": n_splats / (mean_chaos / 1e3) / srate,
             "note": "a splat = 4 saturating u32 atomics on one 16-byte bucket; peak = the same splats "
                     "into uniformly random buckets of this histogram (pyr3_splat_rate), measured here"},
+        "present_roofline": _present_roofline(g, present_ms, peak, peak_kind),
         "gpu_launches": chaos_launches + args.steps * (1 + (1 if g.density is not None else 0)),
         "clocks": clk,
     }
@@ -362,6 +365,24 @@ def bench_ours(args, ws, rank, local, dist):
                                 "sample": sample}
     r.destroy()
     return line
+
+
+def _present_roofline(g, present_ms, peak, peak_kind):
+    """HBM roofline of the present (density estimation when the workload
+    sets it, then tonemap to RGBA8), from its CUDA-event time per step.
+    Algorithmic bytes: the histogram read once (16 B per super-sampled
+    bucket) and the image written (4 B per pixel); with density estimation
+    also the filtered buckets written and read once more (2 x 16 B)."""
+    W, H = g.size
+    n_super = W * H * g.oversample * g.oversample
+    nbytes = n_super * 16 + W * H * 4 + (2 * n_super * 16 if g.density is not None else 0)
+    ms = statistics.mean(present_ms)
+    achieved = nbytes / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "ms": ms, "bytes": nbytes,
+            "note": ("density estimation + tonemap" if g.density is not None else "tonemap") +
+                    f"; the disc spreading of density estimation is bound by shared-memory accumulation, "
+                    f"not HBM; peak {peak_kind}"}
 
 
 def bench_batch(args, ws, rank, local, dist):

@@ -1214,7 +1214,8 @@ static int run_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t to
     d.k1 = k1;
     d.k2 = k2;
     d.R = (int)std::ceil(std::min(std::max(d.max_rad, 0.0f), 256.0f));
-    CUDA_TRY(pyr3::launch_density(r->d_hist, r->d_filtered, d, r->d_knorm, r->d_kwtab, r->stream));
+    CUDA_TRY(pyr3::launch_density(r->d_hist, r->d_filtered, d, r->d_knorm, r->d_kwtab,
+                                  (unsigned long long*)(r->d_sched + 1), r->stream));
     filtered = r->d_filtered;
   }
   pyr3::TonemapParams t;
@@ -1240,7 +1241,7 @@ static int run_present(pyr3_renderer* r, const pyr3_present_opts* p, uint64_t to
   t.hsl_sat = p->hsl_sat;
   t.hsl_light = p->hsl_light;
   CUDA_TRY(pyr3::launch_tonemap(filtered ? nullptr : r->d_hist, filtered, t, r->d_kern, r->d_curves,
-                                dev_out, out_kind, r->stream));
+                                dev_out, out_kind, (unsigned long long*)(r->d_sched + 1), r->stream));
   return PYR3_OK;
 }
 
@@ -1379,12 +1380,14 @@ PYR3_API int pyr3_auto_exposure(pyr3_renderer* r, const pyr3_present_opts* p, ui
 namespace {
 // The queue and wave chaos kernels set sched[1] if one of their bounded
 // waits ran out (a walker-queue wait, or a chunk copy that did not land) or
-// a chunk copy was refused for a misaligned source; it stays set until the
-// next reset.
+// a chunk copy was refused for a misaligned source, and the TMA-staged
+// density and tonemap passes set bits 3 and 4 if a tile's copy did not
+// land; it stays set until the next reset.
 int check_sched(pyr3_renderer* r) {
   uint64_t f = 0;
   CUDA_TRY(cudaMemcpyAsync(&f, r->d_sched + 1, 8, cudaMemcpyDeviceToHost, r->stream));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
+  if (f & 24u) return fail(PYR3_E_CUDA, "present: a density or tonemap tile copy did not land within its bounded wait");
   if (f) return fail(PYR3_E_CUDA, "chaos kernel: a bounded wait (walker queue or chunk copy) exceeded its limit, or a chunk copy was refused");
   return PYR3_OK;
 }
@@ -1686,7 +1689,7 @@ PYR3_API int pyr3_density_tonemap_noalloc(const uint32_t* device_hist, uint32_t 
     d.k1 = k1;
     d.k2 = k2;
     d.R = (int)std::ceil(std::min(std::max(d.max_rad, 0.0f), 256.0f));
-    CUDA_TRY(pyr3::launch_density(device_hist, sc.filtered, d, sc.knorm, sc.kwtab, s));
+    CUDA_TRY(pyr3::launch_density(device_hist, sc.filtered, d, sc.knorm, sc.kwtab, nullptr, s));
     filtered = sc.filtered;
   }
   pyr3::TonemapParams t;
@@ -1710,7 +1713,7 @@ PYR3_API int pyr3_density_tonemap_noalloc(const uint32_t* device_hist, uint32_t 
   t.hsl_sat = p->hsl_sat;
   t.hsl_light = p->hsl_light;
   CUDA_TRY(pyr3::launch_tonemap(filtered ? nullptr : device_hist, filtered, t, sc.kern, sc.curves,
-                                device_out, out_kind, s));
+                                device_out, out_kind, nullptr, s));
   return PYR3_OK;
 }
 

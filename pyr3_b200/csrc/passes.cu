@@ -12,6 +12,11 @@
 // atomics); it streams the buckets of the tile plus an R halo with 128-bit
 // loads, and small discs are splatted by the thread that read them while
 // large discs are queued and splatted cooperatively by a whole warp.
+// For kernel radii up to 31 (k_density_tma) the tile and its halo arrive in
+// shared memory by one TMA tensor copy, every bucket is converted once, and
+// the discs are sorted into radius classes: discs of radius 0-3 are spread
+// as one flat list of (disc, tap) items, so every lane of every warp adds
+// one tap, and larger discs are spread a warp at a time.
 //
 // Tonemap restates the visualize fragment shader (src/shaders/
 // visualize_u32.wgsl:147-248 and visualize_f32.wgsl:162-271): fw x fw
@@ -19,11 +24,13 @@
 // for the raw histogram), flam3 alpha / vibrancy / highlight-power
 // composite, background blend, clamp, then the colour curves (5 x 256 LUT:
 // luma, r, g, b, composite, in the shader's order) and the HSL adjustment.
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include "passes.h"
 
@@ -129,6 +136,198 @@ k_density(const uint4* __restrict__ hist, float4* __restrict__ out, DeParams p,
   for (int q = warp; q < nb; q += kDeThreads / 32) de_disc(big[q], tx0, ty0, acc, tab, knorm, lane, 32);
   __syncthreads();
   for (int i = threadIdx.x; i < kTile * kTile; i += kDeThreads) {
+    const int x = tx0 + (i % kTile), y = ty0 + (i / kTile);
+    if (x < (int)p.width && y < (int)p.height) out[(size_t)y * p.width + x] = acc[i];
+  }
+}
+
+// ------------------------------------------------------------ TMA staging
+// Tensor maps over an image of 16-byte RGBA buckets (u32 histogram or f32
+// filtered sums) as a 3-D tensor: dim 0 the four 32-bit channels, dim 1 x,
+// dim 2 y.  A box always starts at channel 0, so the innermost coordinate
+// is 0 and 16-byte aligned; x and y may lie outside the image (a load
+// fills zeros there).  No multicast: each CTA loads its own box.
+__device__ __forceinline__ uint32_t sh_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void tma_bar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n"
+               "fence.mbarrier_init.release.cluster;\n" ::"r"(sh_addr(bar)) : "memory");
+}
+
+// One thread: announce `bytes` on the barrier and start the box copy at
+// bucket (x, y) into dst (128-byte aligned shared memory).
+__device__ __forceinline__ void tma_load_box(void* dst, const CUtensorMap* tm, int x, int y, uint64_t* bar,
+                                             uint32_t bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n"
+               ::"r"(sh_addr(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+               " [%0], [%1, {%2, %3, %4}], [%5];\n"
+               ::"r"(sh_addr(dst)), "l"(reinterpret_cast<uint64_t>(tm)), "r"(0), "r"(x), "r"(y),
+                 "r"(sh_addr(bar)) : "memory");
+}
+
+// Wait for phase 0 of the barrier; false once kTmaWaitLimit polls pass
+// (a copy that never lands is reported, not waited for forever).
+constexpr uint32_t kTmaWaitLimit = 1u << 24;
+__device__ __forceinline__ bool tma_wait(uint64_t* bar) {
+  for (uint32_t it = 0; it < kTmaWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(sh_addr(bar)) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// ------------------------------------------------ density, TMA-staged tile
+constexpr int kDe2Classes = 5;   // discs of radius 0, 1, 2, 3, and >= 4
+constexpr int kDe2Taps = 48;     // taps of the radius-0..3 discs: 1 + 5 + 13 + 29
+constexpr uint16_t kDe2Skip = 0xffffu;
+
+size_t density_tma_smem(int R) {
+  const size_t side = (size_t)kTile + 2 * (size_t)R, n = side * side;
+  return n * 16 + (size_t)kTile * kTile * 16 + n * 4;
+}
+
+// Shared memory: the (32 + 2R)^2 halo (uint4 buckets, converted in place to
+// the ls-scaled float4 each disc spreads), the 32 x 32 accumulator, the
+// radius of each halo bucket (kDe2Skip: empty, or its disc misses the
+// tile) and the halo indices sorted by radius class.
+__global__ void __launch_bounds__(kDeThreads)
+k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, DeParams p,
+              const float* __restrict__ knorm, const float* __restrict__ tab,
+              unsigned long long* __restrict__ fault) {
+  extern __shared__ __align__(128) unsigned char de_smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int cls_n[kDe2Classes], cls_off[kDe2Classes + 1], cls_cur[kDe2Classes];
+  __shared__ signed char tap_dx[kDe2Taps], tap_dy[kDe2Taps];
+  __shared__ unsigned char tap_d2[kDe2Taps];
+  const int R = p.R, side = kTile + 2 * R, nsrc = side * side;
+  float4* hv = (float4*)de_smem;
+  float4* acc = hv + nsrc;
+  uint16_t* rad = (uint16_t*)(acc + kTile * kTile);
+  uint16_t* idx = rad + nsrc;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
+  const int hx0 = tx0 - R, hy0 = ty0 - R;
+
+  if (t == 0) tma_bar_init(&bar);
+  if (t < kDe2Classes) cls_n[t] = 0;
+  if (t == 32) {  // taps of the discs of radius 0..3, row by row
+    int n = 0;
+    for (int r = 0; r <= 3; ++r)
+      for (int dy = -r; dy <= r; ++dy)
+        for (int dx = -r; dx <= r; ++dx)
+          if (dx * dx + dy * dy <= r * r) {
+            tap_dx[n] = (signed char)dx;
+            tap_dy[n] = (signed char)dy;
+            tap_d2[n] = (unsigned char)(dx * dx + dy * dy);
+            ++n;
+          }
+  }
+  for (int i = t; i < kTile * kTile; i += kDeThreads) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  __syncthreads();
+  if (t == 0) tma_load_box(hv, &tm, hx0, hy0, &bar, (uint32_t)nsrc * 16u);
+  if (!__syncthreads_and(tma_wait(&bar))) {
+    // The copy did not land in time (the whole block agrees): report it,
+    // wait once more (bounded) so no copy still writes this block's shared
+    // memory, and mark the tile NaN rather than leave it stale.
+    if (t == 0 && fault) atomicOr(fault, 8ull);
+    tma_wait(&bar);
+    const float nan = __int_as_float(0x7fc00000);
+    for (int i = t; i < kTile * kTile; i += kDeThreads) {
+      const int x = tx0 + (i % kTile), y = ty0 + (i / kTile);
+      if (x < (int)p.width && y < (int)p.height) out[(size_t)y * p.width + x] = make_float4(nan, nan, nan, nan);
+    }
+    return;
+  }
+
+  // Pass 1: radius, disc test and ls scaling of every halo bucket, in
+  // place; class counts by warp ballots.
+  for (int e0 = warp * 32; e0 < nsrc; e0 += kDeThreads) {
+    const int e = e0 + lane;
+    int cls = -1;
+    if (e < nsrc) {
+      uint16_t rr = kDe2Skip;
+      const float4 hb = hv[e];  // the raw bucket's bits (read and rewritten as float4)
+      const uint4 h = make_uint4(__float_as_uint(hb.x), __float_as_uint(hb.y), __float_as_uint(hb.z),
+                                 __float_as_uint(hb.w));
+      const float nc = (float)h.w;
+      if (nc > 0.0f) {
+        const int sx = hx0 + e % side, sy = hy0 + e / side;
+        const float hits = nc / 255.0f;
+        const float rf = fminf(fmaxf(p.max_rad / powf(hits + 1.0f, p.curve), p.min_rad), p.max_rad);
+        const int r = min(max((int)rintf(rf), 0), 256);
+        if (!(sx + r < tx0 || sx - r > tx0 + kTile - 1 || sy + r < ty0 || sy - r > ty0 + kTile - 1)) {
+          const float ls = (p.k1 * logf(1.0f + nc * p.k2)) / nc;
+          hv[e] = make_float4((float)h.x * ls, (float)h.y * ls, (float)h.z * ls, nc * ls);
+          rr = (uint16_t)r;
+          cls = min(r, kDe2Classes - 1);
+        }
+      }
+      rad[e] = rr;
+    }
+#pragma unroll
+    for (int c = 0; c < kDe2Classes; ++c) {
+      const unsigned m = __ballot_sync(0xffffffffu, cls == c);
+      if (m && lane == __ffs(m) - 1) atomicAdd(&cls_n[c], __popc(m));
+    }
+  }
+  __syncthreads();
+  if (t == 0) {
+    cls_off[0] = 0;
+    for (int c = 0; c < kDe2Classes; ++c) {
+      cls_off[c + 1] = cls_off[c] + cls_n[c];
+      cls_cur[c] = cls_off[c];
+    }
+  }
+  __syncthreads();
+  // Pass 2: halo indices into class order.
+  for (int e0 = warp * 32; e0 < nsrc; e0 += kDeThreads) {
+    const int e = e0 + lane;
+    int cls = -1;
+    if (e < nsrc && rad[e] != kDe2Skip) cls = min((int)rad[e], kDe2Classes - 1);
+#pragma unroll
+    for (int c = 0; c < kDe2Classes; ++c) {
+      const unsigned m = __ballot_sync(0xffffffffu, cls == c);
+      if (!m) continue;
+      const int leader = __ffs(m) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(&cls_cur[c], __popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (cls == c) idx[base + __popc(m & ((1u << lane) - 1u))] = (uint16_t)e;
+    }
+  }
+  __syncthreads();
+  // Discs of radius 0..3: one item per (disc, tap), so all lanes work.
+  const int n0 = cls_n[0], n1 = cls_n[1], n2 = cls_n[2], n3 = cls_n[3];
+  const int e1 = n0, e2 = e1 + 5 * n1, e3 = e2 + 13 * n2, total = e3 + 29 * n3;
+  for (int it = t; it < total; it += kDeThreads) {
+    int c, local, ntap, tap0;
+    if (it < e1) { c = 0; local = it; ntap = 1; tap0 = 0; }
+    else if (it < e2) { c = 1; local = it - e1; ntap = 5; tap0 = 1; }
+    else if (it < e3) { c = 2; local = it - e2; ntap = 13; tap0 = 6; }
+    else { c = 3; local = it - e3; ntap = 29; tap0 = 19; }
+    const int disc = local / ntap, j = tap0 + (local - disc * ntap);
+    const int e = idx[cls_off[c] + disc];
+    const int x = hx0 + e % side + tap_dx[j], y = hy0 + e / side + tap_dy[j];
+    if (x < tx0 || x >= tx0 + kTile || y < ty0 || y >= ty0 + kTile) continue;
+    const float w = tab[kw_offset(c) + tap_d2[j]];
+    const float4 v = hv[e];
+    float* a = (float*)&acc[(y - ty0) * kTile + (x - tx0)];
+    atomicAdd(a + 0, v.x * w);
+    atomicAdd(a + 1, v.y * w);
+    atomicAdd(a + 2, v.z * w);
+    atomicAdd(a + 3, v.w * w);
+  }
+  // Discs of radius >= 4: a warp each.
+  for (int q = warp; q < cls_n[4]; q += kDeThreads / 32) {
+    const int e = idx[cls_off[4] + q];
+    const DeBucket b{hx0 + e % side, hy0 + e / side, (int)rad[e], hv[e]};
+    de_disc(b, tx0, ty0, acc, tab, knorm, lane, 32);
+  }
+  __syncthreads();
+  for (int i = t; i < kTile * kTile; i += kDeThreads) {
     const int x = tx0 + (i % kTile), y = ty0 + (i / kTile);
     if (x < (int)p.width && y < (int)p.height) out[(size_t)y * p.width + x] = acc[i];
   }
@@ -398,15 +597,47 @@ template <bool kU32, int kOut>
 __global__ void __launch_bounds__(256)
 k_tonemap_tile(const uint4* __restrict__ hu, const float4* __restrict__ hf, TonemapParams p,
                const float* __restrict__ kern, const float* __restrict__ curves, void* __restrict__ out,
-               int T, int side) {
-  extern __shared__ float4 tile[];  // side x side
+               int T, int side, const __grid_constant__ CUtensorMap tm, int use_tma,
+               unsigned long long* __restrict__ fault) {
+  extern __shared__ __align__(128) float4 tile[];  // side x side
   __shared__ float kk[kMaxTaps];
+  __shared__ __align__(8) uint64_t bar;
   if (threadIdx.x < p.fwidth) kk[threadIdx.x] = kern[threadIdx.x];
   const int N = (int)p.oversample, fw = (int)p.fwidth, half = fw / 2;
   const int sw = (int)p.width * N, sh = (int)p.height * N;
   const int ox = (int)blockIdx.x * T * N + N / 2 - half, oy = (int)blockIdx.y * T * N + N / 2 - half;
-  // Four loads in flight per thread, then the conversions.
   const int n = side * side, nt = (int)blockDim.x;
+  // A tile whose source square lies inside the image arrives by one TMA
+  // tensor copy (then converted in place); an edge tile, whose taps clamp to
+  // the border, reads its square with clamped loads.
+  if (use_tma && ox >= 0 && oy >= 0 && ox + side <= sw && oy + side <= sh) {
+    if (threadIdx.x == 0) tma_bar_init(&bar);
+    __syncthreads();
+    if (threadIdx.x == 0) tma_load_box(tile, &tm, ox, oy, &bar, (uint32_t)n * 16u);
+    if (!__syncthreads_and(tma_wait(&bar))) {
+      if (threadIdx.x == 0 && fault) atomicOr(fault, 16ull);
+      tma_wait(&bar);
+      const float nan = __int_as_float(0x7fc00000);
+      const float o[4] = {nan, nan, nan, nan};
+      const uint32_t xi = blockIdx.x * T + (int)threadIdx.x % T, yi = blockIdx.y * T + (int)threadIdx.x / T;
+      if (xi < p.width && yi < p.height) store_pixel<kOut>(o, out, (size_t)yi * p.width + xi);
+      return;
+    }
+    if (kU32) {
+      for (int e = threadIdx.x; e < n; e += nt) {
+        const float4 b = tile[e];
+        const float cnt = (float)__float_as_uint(b.w);
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (cnt > 0.0f) {
+          const float ls = (p.k1 * logf(1.0f + cnt * p.k2)) / cnt;
+          v = make_float4((float)__float_as_uint(b.x) * ls, (float)__float_as_uint(b.y) * ls,
+                          (float)__float_as_uint(b.z) * ls, cnt * ls);
+        }
+        tile[e] = v;
+      }
+    }
+  } else
+  // Four loads in flight per thread, then the conversions.
   for (int e0 = threadIdx.x; e0 < n; e0 += 4 * nt) {
     uint4 raw[4];
 #pragma unroll
@@ -469,9 +700,65 @@ cudaError_t build_kw_table(const float* knorm, float* tab, cudaStream_t s) {
 
 size_t kw_table_floats() { return (size_t)(kKwMaxR * (kKwMaxR + 1) * (2 * kKwMaxR + 1)) / 6 + kKwMaxR + 1 + 1; }
 
+namespace {
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links no driver library); null if the driver has none.
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return (EncodeTiledFn)f;
+  }();
+  return fn;
+}
+}  // namespace
+
+bool encode_bucket_map(CUtensorMap* tm, const void* base, uint32_t width, uint32_t height, uint32_t box_w,
+                       uint32_t box_h) {
+  const EncodeTiledFn fn = encode_tiled();
+  if (!fn || ((uintptr_t)base & 15u) || box_w < 1 || box_w > 256 || box_h < 1 || box_h > 256) return false;
+  const cuuint64_t dims[3] = {4, width, height};
+  const cuuint64_t strides[2] = {16, (cuuint64_t)width * 16};
+  const cuuint32_t box[3] = {4, box_w, box_h};
+  const cuuint32_t estride[3] = {1, 1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, const_cast<void*>(base), dims, strides, box, estride,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 cudaError_t launch_density(const uint32_t* hist, float* filtered, const DeParams& p,
-                           const float* knorm, const float* tab, cudaStream_t s) {
+                           const float* knorm, const float* tab, unsigned long long* fault, cudaStream_t s) {
   dim3 grid((p.width + kTile - 1) / kTile, (p.height + kTile - 1) / kTile);
+  // The TMA-staged kernel where its tile fits in shared memory (kernel
+  // radius up to kDensityTmaMaxR); the streaming kernel otherwise.
+  if (p.R >= 0 && p.R <= kDensityTmaMaxR) {
+    CUtensorMap tm;
+    const uint32_t side = (uint32_t)(kTile + 2 * p.R);
+    if (encode_bucket_map(&tm, hist, p.width, p.height, side, side)) {
+      const size_t smem = density_tma_smem(p.R);
+      static bool attr_set[64] = {};  // per device: the attribute belongs to the current device
+      int dev = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e != cudaSuccess) return e;
+      if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+        e = cudaFuncSetAttribute(k_density_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)density_tma_smem(kDensityTmaMaxR));
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
+      }
+      k_density_tma<<<grid, kDeThreads, smem, s>>>(tm, (float4*)filtered, p, knorm, tab, fault);
+      return cudaGetLastError();
+    }
+  }
   k_density<<<grid, kDeThreads, 0, s>>>((const uint4*)hist, (float4*)filtered, p, knorm, tab);
   return cudaGetLastError();
 }
@@ -479,15 +766,23 @@ cudaError_t launch_density(const uint32_t* hist, float* filtered, const DeParams
 namespace {
 template <int kOut>
 void tonemap_launch(const uint32_t* hist_u32, const float* filtered, const TonemapParams& p,
-                    const float* kern, const float* curves, void* out, int T, int side, cudaStream_t s) {
+                    const float* kern, const float* curves, void* out, int T, int side,
+                    unsigned long long* fault, cudaStream_t s) {
   if (T) {
     dim3 grid((p.width + T - 1) / T, (p.height + T - 1) / T);
     const size_t smem = (size_t)side * side * sizeof(float4);
     const unsigned thr = (unsigned)(T * T);
+    CUtensorMap tm;
+    const void* src = hist_u32 ? (const void*)hist_u32 : (const void*)filtered;
+    const int use_tma = encode_bucket_map(&tm, src, p.width * p.oversample, p.height * p.oversample,
+                                          (uint32_t)side, (uint32_t)side) ? 1 : 0;
+    if (!use_tma) std::memset(&tm, 0, sizeof tm);
     if (hist_u32)
-      k_tonemap_tile<true, kOut><<<grid, thr, smem, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out, T, side);
+      k_tonemap_tile<true, kOut><<<grid, thr, smem, s>>>((const uint4*)hist_u32, nullptr, p, kern, curves, out, T,
+                                                         side, tm, use_tma, fault);
     else
-      k_tonemap_tile<false, kOut><<<grid, thr, smem, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out, T, side);
+      k_tonemap_tile<false, kOut><<<grid, thr, smem, s>>>(nullptr, (const float4*)filtered, p, kern, curves, out,
+                                                          T, side, tm, use_tma, fault);
     return;
   }
   dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
@@ -521,7 +816,7 @@ size_t out_bytes_per_pixel(int out_kind) {
 
 cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, const TonemapParams& p,
                            const float* kern, const float* curves, void* out, int out_kind,
-                           cudaStream_t s) {
+                           unsigned long long* fault, cudaStream_t s) {
   // Shared-memory tile of 16 x 16 (else 8 x 8) output pixels when its source
   // square fits in 48 KB; the per-tap gather otherwise (large oversample
   // with a wide filter).
@@ -536,11 +831,11 @@ cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, cons
     }
   }
   switch (out_kind) {
-    case kOutRgba8: tonemap_launch<kOutRgba8>(hist_u32, filtered, p, kern, curves, out, T, side, s); break;
-    case kOutRgba32f: tonemap_launch<kOutRgba32f>(hist_u32, filtered, p, kern, curves, out, T, side, s); break;
-    case kOutRgba16f: tonemap_launch<kOutRgba16f>(hist_u32, filtered, p, kern, curves, out, T, side, s); break;
-    case kOutPng16: tonemap_launch<kOutPng16>(hist_u32, filtered, p, kern, curves, out, T, side, s); break;
-    case kOutExrDisplay: tonemap_launch<kOutExrDisplay>(hist_u32, filtered, p, kern, curves, out, T, side, s); break;
+    case kOutRgba8: tonemap_launch<kOutRgba8>(hist_u32, filtered, p, kern, curves, out, T, side, fault, s); break;
+    case kOutRgba32f: tonemap_launch<kOutRgba32f>(hist_u32, filtered, p, kern, curves, out, T, side, fault, s); break;
+    case kOutRgba16f: tonemap_launch<kOutRgba16f>(hist_u32, filtered, p, kern, curves, out, T, side, fault, s); break;
+    case kOutPng16: tonemap_launch<kOutPng16>(hist_u32, filtered, p, kern, curves, out, T, side, fault, s); break;
+    case kOutExrDisplay: tonemap_launch<kOutExrDisplay>(hist_u32, filtered, p, kern, curves, out, T, side, fault, s); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

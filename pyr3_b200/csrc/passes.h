@@ -40,12 +40,20 @@ size_t out_bytes_per_pixel(int out_kind);
 
 cudaError_t build_kw_table(const float* knorm, float* tab, cudaStream_t s);
 size_t kw_table_floats();
+// Density estimation of a super-res histogram (16-byte aligned) into
+// filtered.  Kernel radii up to kDensityTmaMaxR run the TMA-staged tile
+// kernel, larger ones the streaming kernel.  fault (nullable): bit 3 is set
+// if a tile's copy did not land within its bounded wait (that tile is NaN).
+constexpr int kDensityTmaMaxR = 31;
 cudaError_t launch_density(const uint32_t* hist, float* filtered, const DeParams& p,
-                           const float* knorm, const float* tab, cudaStream_t s);
+                           const float* knorm, const float* tab, unsigned long long* fault, cudaStream_t s);
 // curves: 5 x 256 f32 LUT on the device (read only when p.curves_active != 0).
+// Interior tiles of the shared-memory tile pass arrive by TMA tensor copies
+// (16-byte aligned source); fault (nullable): bit 4 is set if a tile's copy
+// did not land within its bounded wait (that tile's pixels are NaN).
 cudaError_t launch_tonemap(const uint32_t* hist_u32, const float* filtered, const TonemapParams& p,
                            const float* kern, const float* curves, void* out, int out_kind,
-                           cudaStream_t s);
+                           unsigned long long* fault, cudaStream_t s);
 // An rgba32f fragment-value image (16-byte aligned) written as another
 // output kind, with the same per-pixel steps as the tonemap's store.
 cudaError_t launch_convert_display(const float* in, uint64_t pixels, int out_kind, void* out, int sms,

@@ -411,6 +411,43 @@ def test_tonemap_parameter_space_within_1_255(tm, os_, de):
     assert err <= 1.0 / 255.0, err
 
 
+@pytest.mark.parametrize("W,H,os_,max_rad", [(37, 29, 3, 9.0), (8, 6, 1, 9.0), (50, 40, 2, 16.0),
+                                              (70, 45, 1, 30.0)])
+def test_density_paths_within_1_255(W, H, os_, max_rad):
+    """Density estimation on random histograms through both kernels: the
+    TMA-staged tile kernel (kernel radius up to 31: a ragged 37 x 29 canvas
+    at oversample 3, radius 28; an 8 x 6 canvas smaller than one tile;
+    radius 31 at oversample 1) and the streaming kernel (radius 33).
+    Filtered buckets within 1e-4 relative at the 99.9th percentile of the
+    oracle's density_main restatement, the tonemapped image within 1/255."""
+    rng = np.random.default_rng(int(W * 7 + os_))
+    n = W * os_ * H * os_
+    cnt = rng.integers(0, 300, n).astype(np.uint32)
+    cnt[rng.random(n) < 0.35] = 0
+    cnt[rng.random(n) < 0.05] = 40000  # dense buckets: small discs
+    hist = np.zeros((n, 4), np.uint32)
+    hist[:, 3] = cnt * 255
+    for c in range(3):
+        hist[:, c] = (cnt * rng.integers(0, 256, n)).astype(np.uint32)
+    hist = hist.reshape(-1)
+    g = workloads.plain_small()
+    g.scale = W / 4
+    g.density = {"maxRad": max_rad, "minRad": 0.0, "curve": 0.4}
+    samples = int(cnt.sum())
+    p = R.Renderer.present_opts(None, g)
+    out = np.zeros(W * H * 4, np.float32)
+    filt = np.zeros(n * 4, np.float32)
+    _lib.check(_lib.lib().pyr3_density_tonemap(_lib.ptr(hist), W, H, os_, 0.5, C.byref(p), samples,
+                                               _lib.ptr(out), _lib.ptr(filt)))
+    k1, k2 = O.derive_calibration(g.scale, samples, 4.0, os_)
+    ref_f = O.density(hist, W * os_, H * os_, max_rad * os_ + 1, 1.0, 0.4, np.float32(k1), np.float32(k2))
+    rel = np.abs(filt - ref_f) / np.maximum(np.abs(ref_f), 1e-3)
+    assert float(np.percentile(rel, 99.9)) < 1e-4
+    ref = O.visualize(W, H, os_, O.spatial_kernel(0.5, os_), np.float32(k1), np.float32(k2), 4.0, 1.0, 1.0,
+                      0.01, src_f32=ref_f)
+    assert float(np.abs(out - ref).max()) <= 1.0 / 255.0
+
+
 def test_density_radius_31_within_1_255():
     """Density estimation at the motion_4k setting, 15 / 0 / 0.6 at
     oversample 2 (kernel radius 31, 3,969 taps per super-pixel), against
