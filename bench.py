@@ -211,10 +211,15 @@ def bench_ours(args, ws, rank, local, dist):
     g, g_close = _workload(args.config)
     W, H = g.size
     os_ = g.oversample
-    walkers, iters, samples = R.compute_dispatch(g.quality, W, H)
     if args.samples:  # profiling case: same genome and canvas, fewer samples per step
-        walkers, iters = 1024, max(1, args.samples // 1024)
-        samples = walkers * iters
+        import copy
+
+        g = copy.deepcopy(g)
+        g.quality = args.samples / (W * H)
+        if g_close is not None:
+            g_close = copy.deepcopy(g_close)
+            g_close.quality = g.quality
+    walkers, iters, samples = R.compute_dispatch(g.quality, W, H)
     r = R.create_renderer(W, H, os_, g.filter_radius, device=local)
     gg = R.GpuGenome(g)
     r.prepare(gg)  # NVRTC specialisation (cached), outside the timed region
@@ -542,7 +547,7 @@ def bench_denoise(args, ws, rank, local, dist):
     clk = clocks.stop() if clocks else None
     t_max = _max_over_ranks(ms, dist, local)
     p_noisy, p_dn, dn_img = DN.evaluate(net.params(), xho, tho)
-    ssim_in = DN.ssim(np.clip(xho[:, :3], 0.0, 1.0), tho)
+    ssim_in = DN.ssim(np.clip(xho[:, DN.IN_CH:DN.IN_CH + DN.OUT_CH], 0.0, 1.0), tho)
     ssim_dn = DN.ssim(dn_img, tho)
     # time to quality: plain renders of the held-out genomes at rising spp against the
     # same 2000-spp targets, and the denoiser's inference time for all of them
@@ -562,7 +567,7 @@ def bench_denoise(args, ws, rank, local, dist):
     hnet = DN.UNet(batch, crop, crop, net.params())
     hnet.capture()
     n_e2e = per
-    hx = np.empty((batch, 8, crop, crop), np.float32)
+    hx = np.empty((batch, DN.IN_CH + DN.OUT_CH, crop, crop), np.float32)
     ht = np.empty((batch, 3, crop, crop), np.float32)
     torch.cuda.synchronize()
     t0 = _t.perf_counter()

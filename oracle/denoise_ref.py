@@ -108,11 +108,14 @@ def unpack(params, chans, in_ch=8, out_ch=3):
 
 
 def forward(params, x, chans):
-    """Returns (output, cache) for unet_backward."""
+    """Returns (output, cache) for unet_backward.  x holds the feature
+    channels followed by the three channels of the noisy image that the
+    last convolution's output is added to."""
     L = len(chans)
-    layers = unpack(params, chans, x.shape[1])
-    cache = {"x": x, "inp": [], "a": [], "e": [], "cat": [], "da": [], "d": {}}
-    inp = x
+    in_ch = x.shape[1] - 3
+    layers = unpack(params, chans, in_ch)
+    cache = {"x": x, "in_ch": in_ch, "inp": [], "a": [], "e": [], "cat": [], "da": [], "d": {}}
+    inp = x[:, :in_ch]
     li = 0
     for l in range(L):
         if l > 0:
@@ -133,14 +136,14 @@ def forward(params, x, chans):
         cats[l], das[l], cache["d"][l] = cat, da, d
         below = d
     cache["cat"], cache["da"] = cats, das
-    out = conv3x3(cache["d"][0], *layers[li]) + x[:, :3]
+    out = conv3x3(cache["d"][0], *layers[li]) + x[:, in_ch:in_ch + 3]
     return out, cache
 
 
 def backward(params, cache, gout, chans):
     """Gradient of the loss w.r.t. the flat parameters, given d loss / d out."""
     L = len(chans)
-    layers = unpack(params, chans, cache["x"].shape[1])
+    layers = unpack(params, chans, cache["in_ch"])
     grads = [None] * len(layers)
     lo = len(layers) - 1
     dw, db = conv3x3_wgrad(cache["d"][0], gout)

@@ -183,6 +183,7 @@ __device__ __forceinline__ bool tma_wait(uint64_t* bar) {
 constexpr int kDe2Classes = 5;   // discs of radius 0, 1, 2, 3, and >= 4
 constexpr int kDe2Taps = 48;     // taps of the radius-0..3 discs: 1 + 5 + 13 + 29
 constexpr uint16_t kDe2Skip = 0xffffu;
+constexpr int kDe2MaxThreads = 1024;
 
 size_t density_tma_smem(int R) {
   const size_t side = (size_t)kTile + 2 * (size_t)R, n = side * side;
@@ -193,7 +194,7 @@ size_t density_tma_smem(int R) {
 // the ls-scaled float4 each disc spreads), the 32 x 32 accumulator, the
 // radius of each halo bucket (kDe2Skip: empty, or its disc misses the
 // tile) and the halo indices sorted by radius class.
-__global__ void __launch_bounds__(kDeThreads)
+__global__ void __launch_bounds__(kDe2MaxThreads)
 k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, DeParams p,
               const float* __restrict__ knorm, const float* __restrict__ tab,
               unsigned long long* __restrict__ fault) {
@@ -207,7 +208,7 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
   float4* acc = hv + nsrc;
   uint16_t* rad = (uint16_t*)(acc + kTile * kTile);
   uint16_t* idx = rad + nsrc;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nthr = (int)blockDim.x;
   const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
   const int hx0 = tx0 - R, hy0 = ty0 - R;
 
@@ -225,7 +226,7 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
             ++n;
           }
   }
-  for (int i = t; i < kTile * kTile; i += kDeThreads) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = t; i < kTile * kTile; i += nthr) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
   if (t == 0) tma_load_box(hv, &tm, hx0, hy0, &bar, (uint32_t)nsrc * 16u);
   if (!__syncthreads_and(tma_wait(&bar))) {
@@ -235,7 +236,7 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
     if (t == 0 && fault) atomicOr(fault, 8ull);
     tma_wait(&bar);
     const float nan = __int_as_float(0x7fc00000);
-    for (int i = t; i < kTile * kTile; i += kDeThreads) {
+    for (int i = t; i < kTile * kTile; i += nthr) {
       const int x = tx0 + (i % kTile), y = ty0 + (i / kTile);
       if (x < (int)p.width && y < (int)p.height) out[(size_t)y * p.width + x] = make_float4(nan, nan, nan, nan);
     }
@@ -244,7 +245,7 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
 
   // Pass 1: radius, disc test and ls scaling of every halo bucket, in
   // place; class counts by warp ballots.
-  for (int e0 = warp * 32; e0 < nsrc; e0 += kDeThreads) {
+  for (int e0 = warp * 32; e0 < nsrc; e0 += nthr) {
     const int e = e0 + lane;
     int cls = -1;
     if (e < nsrc) {
@@ -283,7 +284,7 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
   }
   __syncthreads();
   // Pass 2: halo indices into class order.
-  for (int e0 = warp * 32; e0 < nsrc; e0 += kDeThreads) {
+  for (int e0 = warp * 32; e0 < nsrc; e0 += nthr) {
     const int e = e0 + lane;
     int cls = -1;
     if (e < nsrc && rad[e] != kDe2Skip) cls = min((int)rad[e], kDe2Classes - 1);
@@ -302,7 +303,7 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
   // Discs of radius 0..3: one item per (disc, tap), so all lanes work.
   const int n0 = cls_n[0], n1 = cls_n[1], n2 = cls_n[2], n3 = cls_n[3];
   const int e1 = n0, e2 = e1 + 5 * n1, e3 = e2 + 13 * n2, total = e3 + 29 * n3;
-  for (int it = t; it < total; it += kDeThreads) {
+  for (int it = t; it < total; it += nthr) {
     int c, local, ntap, tap0;
     if (it < e1) { c = 0; local = it; ntap = 1; tap0 = 0; }
     else if (it < e2) { c = 1; local = it - e1; ntap = 5; tap0 = 1; }
@@ -321,13 +322,13 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
     atomicAdd(a + 3, v.w * w);
   }
   // Discs of radius >= 4: a warp each.
-  for (int q = warp; q < cls_n[4]; q += kDeThreads / 32) {
+  for (int q = warp; q < cls_n[4]; q += nthr / 32) {
     const int e = idx[cls_off[4] + q];
     const DeBucket b{hx0 + e % side, hy0 + e / side, (int)rad[e], hv[e]};
     de_disc(b, tx0, ty0, acc, tab, knorm, lane, 32);
   }
   __syncthreads();
-  for (int i = t; i < kTile * kTile; i += kDeThreads) {
+  for (int i = t; i < kTile * kTile; i += nthr) {
     const int x = tx0 + (i % kTile), y = ty0 + (i / kTile);
     if (x < (int)p.width && y < (int)p.height) out[(size_t)y * p.width + x] = acc[i];
   }
@@ -755,7 +756,10 @@ cudaError_t launch_density(const uint32_t* hist, float* filtered, const DeParams
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) attr_set[dev] = true;
       }
-      k_density_tma<<<grid, kDeThreads, smem, s>>>(tm, (float4*)filtered, p, knorm, tab, fault);
+      // 512 threads where three blocks fit on an SM (48 warps), 1024 where
+      // the halo leaves room for one block only (32 warps).
+      const unsigned thr = smem <= 75 * 1024 ? 512u : 1024u;
+      k_density_tma<<<grid, thr, smem, s>>>(tm, (float4*)filtered, p, knorm, tab, fault);
       return cudaGetLastError();
     }
   }

@@ -13,13 +13,19 @@ Architecture (chans = (16, 24, 32, 40, 48), ~195 k parameters): encoder
 level l = two 3x3 conv + ReLU (input: the features, or the 2x2 average pool
 of level l-1); decoder level l = nearest 2x upsample of the level below
 concatenated with the encoder's level-l output, two 3x3 conv + ReLU; a last
-3x3 conv to 3 channels added to feature channels 0..2 (the noisy image).
+3x3 conv to 3 channels added to the noisy image (the input's last three
+channels, after the features).
 Parameters are one flat f32 vector: per conv, weight [co][ci][3][3] then
 bias[co].  Each encoder output is written straight into its decoder level's
 concatenation buffer, so the skip connection costs no copy.
 
-Features of a render (features()): tonemapped RGB (3), log1p of the linear
-RGB (3), log1p of the bucket count / 255 (1), tonemapped alpha (1).
+Input of a render (features()): 8 feature channels -- log density
+log1p(hits), the normalised RGB accumulators (colour sums / count, 3),
+alpha, the hit count per sample per pixel, the local 3x3 variance of the
+noisy image's luminance, and the density-estimation radius the adaptive
+filter would give the pixel (max_rad / (hits + 1)^curve, clamped, over
+max_rad) -- then the noisy tonemapped RGB (3) as the residual's base.  Hits
+are the pixel's bucket counts / 255 summed over its oversample block.
 """
 from __future__ import annotations
 
@@ -110,7 +116,7 @@ class UNet:
         hs = [(h >> l, w >> l) for l in range(L)]
         self.hs = hs
         z = lambda c, l: torch.zeros((n, c, hs[l][0], hs[l][1]), **f32)  # noqa: E731
-        self.x = z(IN_CH, 0)
+        self.x = z(IN_CH + OUT_CH, 0)  # features, then the noisy image the output is added to
         self.tgt = z(OUT_CH, 0)
         self.out = z(OUT_CH, 0)
         self.gout = z(OUT_CH, 0)
@@ -220,7 +226,7 @@ class UNet:
             i += 2
         o = self._v(self.out)
         self._conv(self._v(self.d[0]), ch[0], o, OUT_CH, 0, i, False)
-        xv = self._v(self.x)
+        xv = self._v(self.x, IN_CH)
         _check(lib.pyr3_dn_add(o[0], o[1], xv[0], xv[1], OUT_CH, self.n, self.h * self.w, st()))
         self.launches += 1
 
@@ -329,18 +335,36 @@ def init_params(chans=CHANS, seed: int = 0) -> np.ndarray:
     return np.concatenate(parts).astype(np.float32)
 
 
+# Density-estimation setting the radius feature is computed with when the
+# genome sets none (the plain_small configuration's 9 / 0 / 0.4).
+FEATURE_DE = {"maxRad": 9.0, "minRad": 0.0, "curve": 0.4}
+
+
 def features(renderer, genome, samples: int) -> np.ndarray:
-    """8 x H x W input features of the renderer's current histogram."""
-    img = renderer.present(genome, samples, fmt="f32").astype(np.float32)  # H x W x 4, 0..1
-    lin = renderer.read_linear(genome, samples)
+    """(IN_CH + OUT_CH) x H x W input of the renderer's current histogram:
+    the 8 feature channels, then the noisy tonemapped RGB."""
+    img = renderer.present(genome, samples, fmt="f32", force_de_off=True).astype(np.float32)  # H x W x 4
+    alpha = renderer.present(genome, samples, fmt="f32", force_de_off=True, transparent=True)[..., 3]
     hist, _, _ = renderer.read_histogram()
-    os_ = renderer.oversample
-    cnt = hist[..., 3].astype(np.float64).reshape(renderer.height, os_, renderer.width, os_).sum(axis=(1, 3))
-    f = np.empty((IN_CH, renderer.height, renderer.width), np.float32)
-    f[0:3] = img[..., :3].transpose(2, 0, 1)
-    f[3:6] = np.log1p(np.maximum(lin[..., :3], 0.0)).transpose(2, 0, 1)
-    f[6] = np.log1p(cnt / 255.0)
-    f[7] = img[..., 3]
+    os_, H, W = renderer.oversample, renderer.height, renderer.width
+    h = hist.astype(np.float64).reshape(H, os_, W, os_, 4).sum(axis=(1, 3))
+    hits = h[..., 3] / 255.0
+    f = np.empty((IN_CH + OUT_CH, H, W), np.float32)
+    f[0] = np.log1p(hits)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        for c in range(3):
+            f[1 + c] = np.where(h[..., 3] > 0, h[..., c] / np.maximum(h[..., 3], 1.0), 0.0)
+    f[4] = alpha
+    f[5] = hits * (W * H) / max(float(samples), 1.0)
+    lum = img[..., 0] * 0.299 + img[..., 1] * 0.587 + img[..., 2] * 0.114
+    pad = np.pad(lum.astype(np.float64), 1, mode="edge")
+    win = np.stack([pad[dy:dy + H, dx:dx + W] for dy in range(3) for dx in range(3)])
+    f[6] = win.var(axis=0)
+    de = genome.density or FEATURE_DE
+    mx, mn = de["maxRad"], de["minRad"]
+    rad = np.clip(mx / np.power(hits + 1.0, de["curve"]), mn, mx)
+    f[7] = np.where(hits > 0, rad / max(mx, 1e-6), 0.0)
+    f[IN_CH:] = img[..., :3].transpose(2, 0, 1)
     return f
 
 
@@ -372,7 +396,7 @@ def psnr(a: np.ndarray, b: np.ndarray) -> float:
 
 
 def make_dataset(genomes, spp_in: float = 25.0, spp_target: float = 2000.0, seed: int = 0):
-    """(inputs N x 8 x H x W, targets N x 3 x H x W) from renders of each
+    """(inputs N x 11 x H x W, targets N x 3 x H x W) from renders of each
     genome at spp_in and spp_target samples per pixel (one renderer)."""
     from . import renderer as R
 
@@ -429,7 +453,7 @@ def evaluate(params, xs, ts, chans=CHANS, tensor_cores: bool = True):
     net.set_batch(xs, ts)
     net.forward()
     out = np.clip(net.output(), 0.0, 1.0)
-    return psnr(np.clip(xs[:, :3], 0.0, 1.0), ts), psnr(out, ts), out
+    return psnr(np.clip(xs[:, IN_CH:IN_CH + OUT_CH], 0.0, 1.0), ts), psnr(out, ts), out
 
 
 def plain_quality(genomes, targets, spps, seed: int = 99):

@@ -18,11 +18,12 @@ CH_SMALL = (4, 6, 8)
 # ------------------------------------------------------------ CPU: oracle pins
 def _torch_unet(params, x, chans):
     L = len(chans)
+    in_ch = x.shape[1] - 3
     layers = [(torch.tensor(w, requires_grad=True), torch.tensor(b, requires_grad=True))
-              for w, b in D.unpack(params, chans, x.shape[1])]
+              for w, b in D.unpack(params, chans, in_ch)]
     xt = torch.tensor(x)
     e = []
-    inp = xt
+    inp = xt[:, :in_ch]
     li = 0
     for l in range(L):
         if l > 0:
@@ -36,7 +37,7 @@ def _torch_unet(params, x, chans):
         da = F.relu(F.conv2d(cat, layers[li][0], layers[li][1], padding=1))
         below = F.relu(F.conv2d(da, layers[li + 1][0], layers[li + 1][1], padding=1))
         li += 2
-    out = F.conv2d(below, layers[li][0], layers[li][1], padding=1) + xt[:, :3]
+    out = F.conv2d(below, layers[li][0], layers[li][1], padding=1) + xt[:, in_ch:in_ch + 3]
     return out, layers
 
 
@@ -72,7 +73,7 @@ def test_oracle_unet_gradient_matches_torch_autograd():
     rng = np.random.default_rng(1)
     params = D.init_params(CH_SMALL, seed=3)
     params[-(3 * 4 * 9 + 3):] = rng.normal(0.0, 0.1, 3 * 4 * 9 + 3)  # non-zero output conv
-    x = rng.normal(size=(2, 8, 16, 16))
+    x = rng.normal(size=(2, 8 + 3, 16, 16))  # 8 feature channels, then the noisy image
     tgt = rng.normal(size=(2, 3, 16, 16))
     out, cache = D.forward(params, x, CH_SMALL)
     loss, gout = D.mse(out, tgt)
@@ -234,7 +235,7 @@ def test_cuda_unet_forward_backward_matches_oracle():
     params = DN.init_params(chans, seed=5)
     params[-(3 * 8 * 9 + 3):] = rng.normal(0.0, 0.05, 3 * 8 * 9 + 3)
     n, h, w = 2, 32, 48
-    x = rng.normal(size=(n, 8, h, w))
+    x = rng.normal(size=(n, DN.IN_CH + DN.OUT_CH, h, w))  # features, then the noisy image
     tgt = rng.normal(size=(n, 3, h, w))
     net = DN.UNet(n, h, w, params, chans=chans, tensor_cores=False)
     net.set_batch(x, tgt)
@@ -277,7 +278,8 @@ def test_adam_training_lowers_the_loss():
     rng = np.random.default_rng(6)
     n, h, w = 2, 32, 32
     clean = rng.uniform(0.0, 1.0, (n, 3, 1, 1)) * np.ones((n, 3, h, w))
-    x = np.concatenate([clean + rng.normal(0.0, 0.2, clean.shape), rng.normal(size=(n, 5, h, w))], axis=1)
+    noisy = clean + rng.normal(0.0, 0.2, clean.shape)
+    x = np.concatenate([noisy, rng.normal(size=(n, 5, h, w)), noisy], axis=1)
     net = DN.UNet(n, h, w, DN.init_params(seed=7))
     net.set_batch(x, clean)
     losses = []

@@ -168,14 +168,20 @@ def _variation_case(idx):
 @pytest.mark.parametrize("case", _impl_ids(), ids=lambda c: c[1])
 def test_variation_matches_reference(case):
     """CUDA variation vs the reference's WGSL (f32, CPU) and vs the same
-    WGSL evaluated in FP64, on a seeded 512-point grid:
+    WGSL evaluated in FP64, on a seeded 512-point grid.  Errors are f32
+    ulps at max(|a|, |b|, 1) (2^-23 relative above 1, absolute below),
+    per point the larger of x and y:
 
-    * relative error (scale max(|a|, |b|, 1)) against the f32 reference
-      <= 1e-3 on at least 99 % of points;
-    * the RNG streams consume identically (same ISAAC state afterwards);
-    * a line of statistics: the f32 ulps (at max(|a|, |b|, 1)) against the
-      f32 reference, max and 99th percentile, and both implementations'
-      error against the FP64 evaluation."""
+    * the RNG streams consume identically on every point (same ISAAC state
+      afterwards);
+    * as accurate as the reference's own f32 shader: the 99th-percentile
+      error against FP64 at most 4x the reference's, or 64 ulps;
+    * agreement with the f32 reference: 99th percentile within 64 ulps or
+      twice the two implementations' FP64 errors (ill-conditioned
+      variations, e.g. the sine hashes, differ by what either is off);
+    * relative error against the f32 reference <= 1e-3 on >= 99 % of
+      points.
+    A line of these statistics is printed per variation."""
     idx, name, _ = case
     pts, p, a0, a1, isaac = _variation_case(idx)
     dev, st_dev = _eval_dev(idx, pts, 0.75, p, a0, a1, isaac)
@@ -190,8 +196,11 @@ def test_variation_matches_reference(case):
     print(f"VARSTAT {name} ulp_vs_ref32 p99 {np.percentile(u32, 99):.4g} max {u32.max():.4g} | "
           f"vs_fp64 dev p99 {np.percentile(u_dev64, 99):.4g} max {u_dev64.max():.4g} "
           f"ref p99 {np.percentile(u_ref64, 99):.4g} max {u_ref64.max():.4g} | same_draws {same_draws:.4f}")
+    p_dev64, p_ref64, p32 = (float(np.percentile(u, 99)) for u in (u_dev64, u_ref64, u32))
+    assert same_draws == 1.0, (name, same_draws)
+    assert p_dev64 <= max(4.0 * p_ref64, 64.0), (name, p_dev64, p_ref64)
+    assert p32 <= max(64.0, 2.0 * (p_dev64 + p_ref64)), (name, p32, p_dev64, p_ref64)
     assert frac_ok >= 0.99, (name, frac_ok, float(np.nanmax(err)))
-    assert same_draws >= 0.99, (name, same_draws)
 
 
 # Variations whose trig takes coordinate- or radius-scaled arguments through
