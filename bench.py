@@ -529,11 +529,13 @@ def bench_denoise(args, ws, rank, local, dist):
     from pyr3_b200 import denoise as DN
     from pyr3_b200 import workloads
 
-    gs = workloads.denoise_set(seed=5 + 1000 * rank, n=72, size=256)
+    n_gen, size, n_ho = args.dn_genomes, args.dn_size, 8
+    gs = workloads.denoise_set(seed=5 + 1000 * rank, n=n_gen, size=size)
     t0 = _t.perf_counter()
     xs, ts = DN.make_dataset(gs)
     render_s = _t.perf_counter() - t0
-    xtr, ttr, xho, tho = xs[:64], ts[:64], xs[64:], ts[64:]
+    n_tr = n_gen - n_ho
+    xtr, ttr, xho, tho = xs[:n_tr], ts[:n_tr], xs[n_tr:], ts[n_tr:]
     per = 200
     batch, crop = 8, 128
     net, _, _ = DN.train(xtr, ttr, steps=per * args.warmup, batch=batch, crop=crop, seed=1)
@@ -551,8 +553,8 @@ def bench_denoise(args, ws, rank, local, dist):
     ssim_dn = DN.ssim(dn_img, tho)
     # time to quality: plain renders of the held-out genomes at rising spp against the
     # same 2000-spp targets, and the denoiser's inference time for all of them
-    plain = DN.plain_quality(gs[64:], tho, (25, 50, 100, 200, 400, 800))
-    inet = DN.UNet(len(xho), 256, 256, net.params())
+    plain = DN.plain_quality(gs[n_tr:], tho, (25, 50, 100, 200, 400, 800))
+    inet = DN.UNet(len(xho), size, size, net.params())
     inet.set_batch(xho)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     inet.forward()
@@ -572,8 +574,8 @@ def bench_denoise(args, ws, rank, local, dist):
     torch.cuda.synchronize()
     t0 = _t.perf_counter()
     for _ in range(n_e2e):
-        idx = rng.integers(0, 64, batch)
-        yy, xx = rng.integers(0, 256 - crop + 1, batch), rng.integers(0, 256 - crop + 1, batch)
+        idx = rng.integers(0, n_tr, batch)
+        yy, xx = rng.integers(0, size - crop + 1, batch), rng.integers(0, size - crop + 1, batch)
         for j in range(batch):
             hx[j] = xtr[idx[j], :, yy[j]:yy[j] + crop, xx[j]:xx[j] + crop]
             ht[j] = ttr[idx[j], :, yy[j]:yy[j] + crop, xx[j]:xx[j] + crop]
@@ -598,10 +600,11 @@ def bench_denoise(args, ws, rank, local, dist):
         "metric": CONFIGS["denoise"][0], "value": value, "unit": "pixels/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (72 seeded genomes, pyr3_b200/workloads.py:denoise_set, rendered here)",
+        "data": f"synthetic ({n_gen} seeded genomes, pyr3_b200/workloads.py:denoise_set, rendered here)",
         "config": {"workload": "denoise", "unet_levels": len(DN.CHANS), "channels": list(DN.CHANS),
-                   "params": DN.param_count(), "canvas": [256, 256], "spp_input": 25, "spp_target": 2000,
-                   "train_genomes": 64, "held_out_genomes": 8, "batch": batch, "crop": crop,
+                   "params": DN.param_count(), "canvas": [size, size], "spp_input": 25, "spp_target": 2000,
+                   "input_channels": DN.IN_CH, "train_genomes": n_tr, "held_out_genomes": n_ho,
+                   "batch": batch, "crop": crop,
                    "adam_steps_per_step": per, "l2": "inputs resident; working set < L2 per layer",
                    "parallelism": f"replicas x{ws}"},
         "quality": {"held_out_psnr_input_db": p_noisy, "held_out_psnr_denoised_db": p_dn,
@@ -849,6 +852,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", default="auto", choices=["auto", "barrier", "queue", "wave"],
                     help="chaos kernel (auto: the autotuner's choice)")
+    ap.add_argument("--dn-genomes", type=int, default=136,
+                    help="denoise: seeded genomes rendered for the dataset (the last 8 held out)")
+    ap.add_argument("--dn-size", type=int, default=384, help="denoise: canvas side of the dataset renders")
     ap.add_argument("--samples", type=int, default=0,
                     help="override samples per step (small profiling case; not a bench number)")
     args = ap.parse_args()
