@@ -538,23 +538,24 @@ def bench_denoise(args, ws, rank, local, dist):
     xtr, ttr, xho, tho = xs[:n_tr], ts[:n_tr], xs[n_tr:], ts[n_tr:]
     per = 200
     batch, crop = 8, 128
-    net, _, _ = DN.train(xtr, ttr, steps=per * args.warmup, batch=batch, crop=crop, seed=1)
+    in_ch = args.dn_input
+    net, _, _ = DN.train(xtr, ttr, steps=per * args.warmup, batch=batch, crop=crop, seed=1, in_ch=in_ch)
     params = net.params()
     torch.cuda.synchronize()
     _barrier(dist)
     clocks = Clocks(local) if rank == 0 else None
     net, losses, ms = DN.train(xtr, ttr, steps=per * args.steps, batch=batch, crop=crop, seed=2,
-                               params=params)
+                               params=params, in_ch=in_ch)
     launches = net.launches
     clk = clocks.stop() if clocks else None
     t_max = _max_over_ranks(ms, dist, local)
-    p_noisy, p_dn, dn_img = DN.evaluate(net.params(), xho, tho)
+    p_noisy, p_dn, dn_img = DN.evaluate(net.params(), xho, tho, in_ch=in_ch)
     ssim_in = DN.ssim(np.clip(xho[:, DN.IN_CH:DN.IN_CH + DN.OUT_CH], 0.0, 1.0), tho)
     ssim_dn = DN.ssim(dn_img, tho)
     # time to quality: plain renders of the held-out genomes at rising spp against the
     # same 2000-spp targets, and the denoiser's inference time for all of them
     plain = DN.plain_quality(gs[n_tr:], tho, (25, 50, 100, 200, 400, 800))
-    inet = DN.UNet(len(xho), size, size, net.params())
+    inet = DN.UNet(len(xho), size, size, net.params(), in_ch=in_ch)
     inet.set_batch(xho)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     inet.forward()
@@ -566,7 +567,7 @@ def bench_denoise(args, ws, rank, local, dist):
     match = next((p for p in plain if p[1] >= p_dn), None)
     # e2e: batches assembled on the host, uploaded each step, loss read back each step
     rng = np.random.default_rng(3)
-    hnet = DN.UNet(batch, crop, crop, net.params())
+    hnet = DN.UNet(batch, crop, crop, net.params(), in_ch=in_ch)
     hnet.capture()
     n_e2e = per
     hx = np.empty((batch, DN.IN_CH + DN.OUT_CH, crop, crop), np.float32)
@@ -589,7 +590,7 @@ def bench_denoise(args, ws, rank, local, dist):
         return None
     pix_step = batch * crop * crop
     value = ws * pix_step * per * args.steps / (t_max / 1e3)
-    flop_pix = 3.0 * DN.flops_per_pixel()  # forward + data and weight gradients
+    flop_pix = 3.0 * DN.flops_per_pixel(in_ch=in_ch)  # forward + data and weight gradients
     achieved = value / ws * flop_pix / 1e12
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -602,8 +603,8 @@ def bench_denoise(args, ws, rank, local, dist):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": f"synthetic ({n_gen} seeded genomes, pyr3_b200/workloads.py:denoise_set, rendered here)",
         "config": {"workload": "denoise", "unet_levels": len(DN.CHANS), "channels": list(DN.CHANS),
-                   "params": DN.param_count(), "canvas": [size, size], "spp_input": 25, "spp_target": 2000,
-                   "input_channels": DN.IN_CH, "train_genomes": n_tr, "held_out_genomes": n_ho,
+                   "params": DN.param_count(in_ch=in_ch), "canvas": [size, size], "spp_input": 25, "spp_target": 2000,
+                   "input_channels": in_ch, "train_genomes": n_tr, "held_out_genomes": n_ho,
                    "batch": batch, "crop": crop,
                    "adam_steps_per_step": per, "l2": "inputs resident; working set < L2 per layer",
                    "parallelism": f"replicas x{ws}"},
@@ -855,6 +856,8 @@ def main():
     ap.add_argument("--dn-genomes", type=int, default=136,
                     help="denoise: seeded genomes rendered for the dataset (the last 8 held out)")
     ap.add_argument("--dn-size", type=int, default=384, help="denoise: canvas side of the dataset renders")
+    ap.add_argument("--dn-input", type=int, default=8, choices=[8, 11],
+                    help="denoise: network input channels: the 8 features, or 11 with the noisy RGB")
     ap.add_argument("--samples", type=int, default=0,
                     help="override samples per step (small profiling case; not a bench number)")
     args = ap.parse_args()

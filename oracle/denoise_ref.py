@@ -107,12 +107,13 @@ def unpack(params, chans, in_ch=8, out_ch=3):
     return out
 
 
-def forward(params, x, chans):
+def forward(params, x, chans, in_ch=None):
     """Returns (output, cache) for unet_backward.  x holds the feature
     channels followed by the three channels of the noisy image that the
-    last convolution's output is added to."""
+    last convolution's output is added to; the first convolution reads
+    channels 0..in_ch-1 (default: the features only)."""
     L = len(chans)
-    in_ch = x.shape[1] - 3
+    in_ch = x.shape[1] - 3 if in_ch is None else in_ch
     layers = unpack(params, chans, in_ch)
     cache = {"x": x, "in_ch": in_ch, "inp": [], "a": [], "e": [], "cat": [], "da": [], "d": {}}
     inp = x[:, :in_ch]
@@ -136,7 +137,7 @@ def forward(params, x, chans):
         cats[l], das[l], cache["d"][l] = cat, da, d
         below = d
     cache["cat"], cache["da"] = cats, das
-    out = conv3x3(cache["d"][0], *layers[li]) + x[:, in_ch:in_ch + 3]
+    out = conv3x3(cache["d"][0], *layers[li]) + x[:, x.shape[1] - 3:]
     return out, cache
 
 

@@ -41,6 +41,21 @@ def _raw(s: str) -> str:
     return "\n".join(parts) if parts else '""'
 
 
+_DRAWS = re.compile(r"\b(RAND01|RAND11|IRAND|rand01|rand_11|irand)\s*\(|[(,]\s*c\s*[),]")
+
+
+def rng_variations(vsrc=None) -> set:
+    """Names of the library's variations that may draw from the walker's
+    random stream: every VAR body that uses an RNG macro or passes the
+    context (which holds the stream) to another function.  The rest draw
+    nothing, whatever their parameters."""
+    if vsrc is None:
+        vsrc = [open(f).read() for f in sorted(glob.glob(os.path.join(JIT, "vlib_*.cuh")))
+                if not f.endswith("vlib_core.cuh")]
+    parts = re.split(r"^(VAR|DCV)\((\w+)\)", "\n".join(vsrc), flags=re.M)
+    return {parts[i + 1] for i in range(1, len(parts), 3) if parts[i] == "VAR" and _DRAWS.search(parts[i + 2])}
+
+
 def generate_sources() -> str:
     os.makedirs(GEN, exist_ok=True)
     core = _strip(open(os.path.join(JIT, "vlib_core.cuh")).read())
@@ -73,6 +88,9 @@ def generate_sources() -> str:
                ", ".join("1" if n in impl else "0" for n in names) + "};")
     out.append("static const unsigned char kVarDc[326] = {" +
                ", ".join("1" if n in dcs else "0" for n in names) + "};")
+    draws = rng_variations(vsrc)
+    out.append("static const unsigned char kVarRng[326] = {" +
+               ", ".join("1" if n in draws else "0" for n in names) + "};")
     text = "\n".join(out) + "\n"
     path = os.path.join(GEN, "jit_sources.inc")
     if not os.path.exists(path) or open(path).read() != text:

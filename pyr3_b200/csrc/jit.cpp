@@ -222,8 +222,14 @@ namespace {
 std::string gen_chaos_source(const GenomeShape& s, int wpb, bool aggregate) {
   const int nxf = (int)s.xf.size();
   std::ostringstream o;
+  // A final xform whose variations draw nothing may be skipped while a
+  // walker burns in (its result is not splatted then); with an opacity gate
+  // below 1 it still runs, since the gate draws.
+  bool final_rng_free = s.has_final;
+  for (int v : s.fin.vars) final_rng_free = final_rng_free && !variation_draws(v);
   o << "#define NXF " << nxf << "\n#define WPB " << wpb << "\n#define HAS_FINAL "
-    << (s.has_final ? 1 : 0) << "\n#define FINAL_SLOT " << nxf << "\n#define PICK_LINEAR "
+    << (s.has_final ? 1 : 0) << "\n#define FINAL_RNG_FREE " << (final_rng_free ? 1 : 0)
+    << "\n#define FINAL_SLOT " << nxf << "\n#define PICK_LINEAR "
     << (nxf <= 16 ? 1 : 0) << "\n#define AGGREGATE " << (aggregate ? 1 : 0) << "\n#define QUEUE "
     << (use_queue(nxf) ? 1 : 0) << "\n#define QWARPS " << kQueueWarps << "\n#define WAVE "
     << (use_wave(nxf) ? 1 : 0) << "\n#define WAVE_MINB " << kWaveMinBlocks << "\n";
@@ -258,6 +264,9 @@ const char* variation_name(int idx) {
   return idx >= 0 && idx < kNumVariations ? kVarNames[idx] : "?";
 }
 bool variation_is_dc(int idx) { return idx >= 0 && idx < kNumVariations && kVarDc[idx] != 0; }
+// True if the variation may draw from the walker's random stream (pre_blur,
+// index 97, always draws; a scan of the library's sources marks the rest).
+bool variation_draws(int idx) { return idx == 97 || (idx >= 0 && idx < kNumVariations && kVarRng[idx] != 0); }
 
 std::string GenomeShape::key() const {
   std::ostringstream o;

@@ -112,5 +112,7 @@ int get_eval_module(int idx, std::shared_ptr<EvalModule>* out, std::string* err)
 bool variation_implemented(int idx);
 const char* variation_name(int idx);
 bool variation_is_dc(int idx);
+// True if the variation may draw from the walker's random stream.
+bool variation_draws(int idx);
 
 }  // namespace pyr3

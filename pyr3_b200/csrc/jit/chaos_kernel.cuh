@@ -32,6 +32,9 @@
 #ifndef MAXRANK
 #define MAXRANK (NXF + 1)
 #endif
+#ifndef FINAL_RNG_FREE
+#define FINAL_RNG_FREE 0
+#endif
 
 __constant__ float c_xf[(NXF + HAS_FINAL) * 116];
 
@@ -360,6 +363,9 @@ VDEV float3 accept_step(const ChaosArgs& A, const float4* pal, const Rng& rng, i
     const float* F = c_xf + FINAL_SLOT * 116;
     bool apply = true;
     if (F[10] != 1.0f) apply = rand01(rng) < F[10];
+    // During the burn-in the final xform's output is not splatted; one that
+    // draws nothing (and has no gate, which draws) need not run at all.
+    else if (FINAL_RNG_FREE && !past_fuse) apply = false;
     if (apply) {
       Ctx cf;
       cf.rng = rng;
@@ -562,6 +568,7 @@ chaos_kernel(const __grid_constant__ ChaosArgs A) {
             const float* F = c_xf + FINAL_SLOT * 116;
             bool apply = true;
             if (F[10] != 1.0f) apply = rand01(rng) < F[10];
+            else if (FINAL_RNG_FREE && i < A.fuse) apply = false;  // not splatted, draws nothing
             if (apply) {
               Ctx cf;
               cf.rng = rng;

@@ -65,7 +65,11 @@ struct DeBucket {
   float4 v;  // hist RGBA * ls
 };
 
-__device__ __forceinline__ void de_disc(const DeBucket& b, int tx0, int ty0, float4* acc,
+// Accumulators of a tile: four planes (R, G, B, A) of kTile x kTile floats,
+// so lanes adding into consecutive pixels of a row hit consecutive banks.
+constexpr int kPlane = kTile * kTile;
+
+__device__ __forceinline__ void de_disc(const DeBucket& b, int tx0, int ty0, float* acc,
                                         const float* __restrict__ tab, const float* __restrict__ knorm,
                                         int lane, int step) {
   // footprint of the disc clipped to the tile
@@ -85,22 +89,22 @@ __device__ __forceinline__ void de_disc(const DeBucket& b, int tx0, int ty0, flo
     const int d2 = dx * dx + dy * dy;
     if (d2 > r2) continue;
     const float w = row ? row[d2] : expf(-(float)d2 / (2.0f * sig * sig)) / kn;
-    float* a = (float*)&acc[(y - ty0) * kTile + (x - tx0)];
-    atomicAdd(a + 0, b.v.x * w);
-    atomicAdd(a + 1, b.v.y * w);
-    atomicAdd(a + 2, b.v.z * w);
-    atomicAdd(a + 3, b.v.w * w);
+    float* a = acc + (y - ty0) * kTile + (x - tx0);
+    atomicAdd(a, b.v.x * w);
+    atomicAdd(a + kPlane, b.v.y * w);
+    atomicAdd(a + 2 * kPlane, b.v.z * w);
+    atomicAdd(a + 3 * kPlane, b.v.w * w);
   }
 }
 
 __global__ void __launch_bounds__(kDeThreads)
 k_density(const uint4* __restrict__ hist, float4* __restrict__ out, DeParams p,
           const float* __restrict__ knorm, const float* __restrict__ tab) {
-  __shared__ float4 acc[kTile * kTile];
+  __shared__ float acc[4 * kPlane];
   __shared__ DeBucket big[kBigQueue];
   __shared__ int n_big;
   const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
-  for (int i = threadIdx.x; i < kTile * kTile; i += kDeThreads) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = threadIdx.x; i < 4 * kPlane; i += kDeThreads) acc[i] = 0.0f;
   if (threadIdx.x == 0) n_big = 0;
   __syncthreads();
 
@@ -137,7 +141,8 @@ k_density(const uint4* __restrict__ hist, float4* __restrict__ out, DeParams p,
   __syncthreads();
   for (int i = threadIdx.x; i < kTile * kTile; i += kDeThreads) {
     const int x = tx0 + (i % kTile), y = ty0 + (i / kTile);
-    if (x < (int)p.width && y < (int)p.height) out[(size_t)y * p.width + x] = acc[i];
+    if (x < (int)p.width && y < (int)p.height)
+      out[(size_t)y * p.width + x] = make_float4(acc[i], acc[kPlane + i], acc[2 * kPlane + i], acc[3 * kPlane + i]);
   }
 }
 
@@ -191,10 +196,10 @@ size_t density_tma_smem(int R) {
 }
 
 // Shared memory: the (32 + 2R)^2 halo (uint4 buckets, converted in place to
-// the ls-scaled float4 each disc spreads), the 32 x 32 accumulator, the
+// the ls-scaled float4 each disc spreads), the 32 x 32 accumulator planes, the
 // radius of each halo bucket (kDe2Skip: empty, or its disc misses the
 // tile) and the halo indices sorted by radius class.
-__global__ void __launch_bounds__(kDe2MaxThreads)
+__global__ void __launch_bounds__(kDe2MaxThreads, 1)
 k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, DeParams p,
               const float* __restrict__ knorm, const float* __restrict__ tab,
               unsigned long long* __restrict__ fault) {
@@ -205,8 +210,8 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
   __shared__ unsigned char tap_d2[kDe2Taps];
   const int R = p.R, side = kTile + 2 * R, nsrc = side * side;
   float4* hv = (float4*)de_smem;
-  float4* acc = hv + nsrc;
-  uint16_t* rad = (uint16_t*)(acc + kTile * kTile);
+  float* acc = (float*)(hv + nsrc);
+  uint16_t* rad = (uint16_t*)(acc + 4 * kPlane);
   uint16_t* idx = rad + nsrc;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nthr = (int)blockDim.x;
   const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
@@ -226,7 +231,7 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
             ++n;
           }
   }
-  for (int i = t; i < kTile * kTile; i += nthr) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = t; i < 4 * kPlane; i += nthr) acc[i] = 0.0f;
   __syncthreads();
   if (t == 0) tma_load_box(hv, &tm, hx0, hy0, &bar, (uint32_t)nsrc * 16u);
   if (!__syncthreads_and(tma_wait(&bar))) {
@@ -315,11 +320,11 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
     if (x < tx0 || x >= tx0 + kTile || y < ty0 || y >= ty0 + kTile) continue;
     const float w = tab[kw_offset(c) + tap_d2[j]];
     const float4 v = hv[e];
-    float* a = (float*)&acc[(y - ty0) * kTile + (x - tx0)];
-    atomicAdd(a + 0, v.x * w);
-    atomicAdd(a + 1, v.y * w);
-    atomicAdd(a + 2, v.z * w);
-    atomicAdd(a + 3, v.w * w);
+    float* a = acc + (y - ty0) * kTile + (x - tx0);
+    atomicAdd(a, v.x * w);
+    atomicAdd(a + kPlane, v.y * w);
+    atomicAdd(a + 2 * kPlane, v.z * w);
+    atomicAdd(a + 3 * kPlane, v.w * w);
   }
   // Discs of radius >= 4: a warp each.
   for (int q = warp; q < cls_n[4]; q += nthr / 32) {
@@ -328,9 +333,10 @@ k_density_tma(const __grid_constant__ CUtensorMap tm, float4* __restrict__ out, 
     de_disc(b, tx0, ty0, acc, tab, knorm, lane, 32);
   }
   __syncthreads();
-  for (int i = t; i < kTile * kTile; i += nthr) {
+  for (int i = t; i < kPlane; i += nthr) {
     const int x = tx0 + (i % kTile), y = ty0 + (i / kTile);
-    if (x < (int)p.width && y < (int)p.height) out[(size_t)y * p.width + x] = acc[i];
+    if (x < (int)p.width && y < (int)p.height)
+      out[(size_t)y * p.width + x] = make_float4(acc[i], acc[kPlane + i], acc[2 * kPlane + i], acc[3 * kPlane + i]);
   }
 }
 

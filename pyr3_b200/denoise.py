@@ -36,7 +36,8 @@ import numpy as np
 from . import _lib
 
 CHANS = (16, 24, 32, 40, 48)
-IN_CH, OUT_CH = 8, 3
+IN_CH, OUT_CH = 8, 3  # feature channels, output (and noisy-image) channels
+IN_CH_WITH_RGB = IN_CH + OUT_CH  # a network may also read the noisy image as input
 
 
 def layer_shapes(chans=CHANS, in_ch=IN_CH, out_ch=OUT_CH):
@@ -51,15 +52,15 @@ def layer_shapes(chans=CHANS, in_ch=IN_CH, out_ch=OUT_CH):
     return shapes
 
 
-def param_count(chans=CHANS):
-    return sum(co * ci * 9 + co for co, ci in layer_shapes(chans))
+def param_count(chans=CHANS, in_ch=IN_CH):
+    return sum(co * ci * 9 + co for co, ci in layer_shapes(chans, in_ch))
 
 
-def flops_per_pixel(chans=CHANS):
+def flops_per_pixel(chans=CHANS, in_ch=IN_CH):
     """Multiply-adds x 2 of one forward pass per full-resolution pixel."""
     f = 0.0
     L = len(chans)
-    shapes = layer_shapes(chans)
+    shapes = layer_shapes(chans, in_ch)
     for i, (co, ci) in enumerate(shapes):
         if i < 2 * L:
             lvl = i // 2
@@ -76,12 +77,14 @@ def _check(rc):
 
 
 class UNet:
-    """Device-resident U-Net for images of N x IN_CH x H x W (H, W multiples
-    of 2^(levels-1)).  forward() then backward() computes the parameter
+    """Device-resident U-Net for images of N x (IN_CH + OUT_CH) x H x W (H, W
+    multiples of 2^(levels-1)): the first convolution reads channels
+    0..in_ch-1 (the features, and with in_ch = IN_CH_WITH_RGB also the noisy
+    image), and the output is added to channels IN_CH..IN_CH+2.  forward() then backward() computes the parameter
     gradient of the MSE against a target; step() applies Adam."""
 
     def __init__(self, n: int, h: int, w: int, params: np.ndarray, chans=CHANS, device: int = 0,
-                 tensor_cores: bool = True):
+                 tensor_cores: bool = True, in_ch: int = IN_CH):
         import torch
 
         if not torch.cuda.is_available():
@@ -94,7 +97,10 @@ class UNet:
         self.dev = torch.device("cuda", device)
         self.n, self.h, self.w, self.chans = n, h, w, tuple(chans)
         self.L = L
-        self.shapes = layer_shapes(chans)
+        if in_ch not in (IN_CH, IN_CH_WITH_RGB):
+            raise ValueError(f"in_ch must be {IN_CH} or {IN_CH_WITH_RGB}")
+        self.in_ch = in_ch  # input channels the first convolution reads, from channel 0
+        self.shapes = layer_shapes(chans, in_ch)
         self.offs = []
         o = 0
         for co, ci in self.shapes:
@@ -210,7 +216,7 @@ class UNet:
                 v = self._v(self.inp[l])
                 _check(lib.pyr3_dn_pool2(e[0], e[1], v[0], v[1], ch[l - 1], self.n, h[0], h[1], 0, 0, st()))
                 self.launches += 1
-            cin = IN_CH if l == 0 else ch[l - 1]
+            cin = self.in_ch if l == 0 else ch[l - 1]
             self._conv(self._v(self.inp[l]), cin, self._v(self.a[l]), ch[l], l, i, True)
             self._conv(self._v(self.a[l]), ch[l], self._e(l), ch[l], l, i + 1, True)
             i += 2
@@ -270,7 +276,7 @@ class UNet:
             ga = self._v(self.gtmp[l])
             self._dgrad(ge, ch[l], ga, ch[l], l, i + 1)
             self._mask(ga, self._v(self.a[l]), ch[l], l)
-            cin = IN_CH if l == 0 else ch[l - 1]
+            cin = self.in_ch if l == 0 else ch[l - 1]
             self._wgrad(self._v(self.inp[l]), cin, ga, ch[l], l, i)
             if l > 0:
                 gi = self._v(self.ginp[l])
@@ -323,12 +329,12 @@ class UNet:
         return self.out.cpu().numpy()
 
 
-def init_params(chans=CHANS, seed: int = 0) -> np.ndarray:
+def init_params(chans=CHANS, seed: int = 0, in_ch: int = IN_CH) -> np.ndarray:
     """He-normal weights, zero biases; the last conv starts at zero, so the
     untrained network returns the noisy image."""
     rng = np.random.default_rng(seed)
     parts = []
-    shapes = layer_shapes(chans)
+    shapes = layer_shapes(chans, in_ch)
     for i, (co, ci) in enumerate(shapes):
         std = 0.0 if i == len(shapes) - 1 else np.sqrt(2.0 / (ci * 9))
         parts += [rng.normal(0.0, 1.0, co * ci * 9) * std, np.zeros(co)]
@@ -414,7 +420,7 @@ def make_dataset(genomes, spp_in: float = 25.0, spp_target: float = 2000.0, seed
 
 
 def train(xs, ts, steps: int = 300, batch: int = 8, crop: int = 128, lr: float = 1e-3, seed: int = 0,
-          chans=CHANS, params=None):
+          chans=CHANS, params=None, in_ch: int = IN_CH):
     """Adam on random crops of (xs, ts), all on the device.  Returns (net,
     losses, device ms of the training steps)."""
     import torch
@@ -424,7 +430,8 @@ def train(xs, ts, steps: int = 300, batch: int = 8, crop: int = 128, lr: float =
     X = torch.tensor(xs, device=dev)
     T = torch.tensor(ts, device=dev)
     n, _, H, W = xs.shape
-    net = UNet(batch, crop, crop, init_params(chans, seed) if params is None else params, chans=chans)
+    net = UNet(batch, crop, crop, init_params(chans, seed, in_ch) if params is None else params, chans=chans,
+               in_ch=in_ch)
     net.capture()
     net.launches = 0
     losses = []
@@ -445,11 +452,11 @@ def train(xs, ts, steps: int = 300, batch: int = 8, crop: int = 128, lr: float =
     return net, losses, e0.elapsed_time(e1)
 
 
-def evaluate(params, xs, ts, chans=CHANS, tensor_cores: bool = True):
+def evaluate(params, xs, ts, chans=CHANS, tensor_cores: bool = True, in_ch: int = IN_CH):
     """(PSNR of the noisy input, PSNR of the denoised output) against the
     targets, over all images, and the denoised images."""
     n, _, H, W = xs.shape
-    net = UNet(n, H, W, params, chans=chans, tensor_cores=tensor_cores)
+    net = UNet(n, H, W, params, chans=chans, tensor_cores=tensor_cores, in_ch=in_ch)
     net.set_batch(xs, ts)
     net.forward()
     out = np.clip(net.output(), 0.0, 1.0)

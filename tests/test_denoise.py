@@ -227,23 +227,27 @@ def test_cuda_layers_match_oracle():
 
 
 @pytest.mark.gpu
-def test_cuda_unet_forward_backward_matches_oracle():
+@pytest.mark.parametrize("in_ch", [8, 11])
+def test_cuda_unet_forward_backward_matches_oracle(in_ch):
+    """The whole U-Net's output and parameter gradient against the numpy
+    oracle, reading the 8 feature channels, or those and the noisy image
+    (11); the output is added to the noisy image either way."""
     from pyr3_b200 import denoise as DN
 
     chans = (8, 12, 16)
     rng = np.random.default_rng(4)
-    params = DN.init_params(chans, seed=5)
+    params = DN.init_params(chans, seed=5, in_ch=in_ch)
     params[-(3 * 8 * 9 + 3):] = rng.normal(0.0, 0.05, 3 * 8 * 9 + 3)
     n, h, w = 2, 32, 48
     x = rng.normal(size=(n, DN.IN_CH + DN.OUT_CH, h, w))  # features, then the noisy image
     tgt = rng.normal(size=(n, 3, h, w))
-    net = DN.UNet(n, h, w, params, chans=chans, tensor_cores=False)
+    net = DN.UNet(n, h, w, params, chans=chans, tensor_cores=False, in_ch=in_ch)
     net.set_batch(x, tgt)
     net.forward()
     net.loss_and_grad()
     net.backward()
     torch.cuda.synchronize()
-    out, cache = D.forward(params.astype(np.float64), x, chans)
+    out, cache = D.forward(params.astype(np.float64), x, chans, in_ch=in_ch)
     loss, gout = D.mse(out, tgt)
     grad = D.backward(params.astype(np.float64), cache, gout, chans)
     _close(net.output(), out, rtol=1e-4, atol=1e-4)
@@ -258,7 +262,7 @@ def test_cuda_unet_forward_backward_matches_oracle():
     torch.cuda.synchronize()
     assert np.array_equal(net.grads(), got.astype(np.float32))
     # the tensor-core network (bf16 operands, f32 accumulation) stays close
-    tcn = DN.UNet(n, h, w, params, chans=chans, tensor_cores=True)
+    tcn = DN.UNet(n, h, w, params, chans=chans, tensor_cores=True, in_ch=in_ch)
     tcn.set_batch(x, tgt)
     tcn.forward()
     tcn.loss_and_grad()

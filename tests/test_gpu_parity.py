@@ -883,7 +883,7 @@ def test_splat_rate_deposits_every_splat():
 
 
 # ------------------------------------- bit-exact against the reference loop
-def _exact_genome():
+def _exact_genome(final_opacity=0.6):
     """Six affine xforms (linear variation) with what the chain does besides
     the variations: post affines, pre_blur (variation 97, five draws and a
     cos / sin each), opacity below 1 on two xforms, a xaos matrix with a
@@ -905,7 +905,7 @@ def _exact_genome():
                           post=tuple(float(v) for v in rng.uniform(-0.9, 0.9, 6)) if k in (0, 3, 4) else None))
     xs[2].xaos[4] = 0.0
     fin = G.Xform(a=0.85, b=0.12, c=0.05, d=-0.1, e=0.9, f=0.02, weight=0.0, color=0.3,
-                  color_speed=0.2, variations=[G.Variation(lin, 1.0)], opacity=0.6,
+                  color_speed=0.2, variations=[G.Variation(lin, 1.0)], opacity=final_opacity,
                   post=(0.95, -0.05, 0.01, 0.04, 1.02, -0.03))
     g = workloads.plain_small()
     g.xforms, g.finalxform = xs, fin
@@ -913,17 +913,20 @@ def _exact_genome():
     return g
 
 
+@pytest.mark.parametrize("final_gate", [True, False])
 @pytest.mark.parametrize("kernel", ["barrier", "wave", "queue"])
-def test_kernels_equal_reference_chaos_main_bit_exact(kernel):
+def test_kernels_equal_reference_chaos_main_bit_exact(kernel, final_gate):
     """chaos_main (chaos.wgsl:8269-8731) on the reference's own walker
     streams: 1024 walkers seeded as packIsaacStates does, 3000 post-fuse
     iterations each, on the genome of _exact_genome (post affines,
-    pre_blur, opacity, xaos, final xform with its opacity gate).  Each
-    CUDA chaos kernel with exact walkers gives the reference's histogram
-    bit for bit, and the same sample and in-canvas counts."""
+    pre_blur, opacity, xaos, a final xform behind an opacity gate below 1,
+    or without a gate, in which case its draw-free chain is skipped during
+    the burn-in).  Each CUDA chaos kernel with exact walkers gives the
+    reference's histogram bit for bit, and the same sample and in-canvas
+    counts."""
     from refrender import chaos as ref_chaos
 
-    g = _exact_genome()
+    g = _exact_genome(0.6 if final_gate else None)
     W, H, walkers, iters = 320, 240, 1024, 3000
     ref = ref_chaos(g, W, H, iters, walkers, seed=9)
     r = R.create_renderer(W, H, 1)

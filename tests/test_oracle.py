@@ -271,3 +271,35 @@ def test_visualize_parameter_space_restatement_matches_reference(tm):
         assert np.array_equal(v1, O.ref_visualize(*args, src_u32=hist, **kw))
         a = O.density(hist, W, H, 9.0 * os_ + 1, 1.0, 0.4, k1, k2)
         assert np.array_equal(O.visualize(*args, src_f32=a, **kw), O.ref_visualize(*args, src_f32=a, **kw))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference shaders not compiled here")
+def test_draw_free_variations_draw_nothing_in_the_reference():
+    """The build marks which variations may draw from the walker's stream
+    (pyr3_b200.build.rng_variations, used to skip a draw-free final xform
+    during the burn-in).  Every variation the library marks draw-free
+    leaves the ISAAC state unchanged in the reference's apply_variation
+    (chaos.wgsl:7731) on a seeded grid with random parameters."""
+    from pyr3_b200 import build as B, genome as G
+
+    draws = B.rng_variations()
+    cat = G.catalog()
+    wrong = []
+    for v in cat:
+        if v["name"] in draws or v["dc"] or v["idx"] == 97:
+            continue
+        rng = np.random.default_rng(v["idx"])
+        pts = rng.uniform(-2.0, 2.0, (256, 2)).astype(np.float32)
+        p = np.zeros(10, np.float32)
+        for k, rg in enumerate(v["ranges"][:10]):
+            if rg:
+                p[k] = rng.uniform(rg[0], rg[1]) if rg[1] > rg[0] else rg[0]
+        a0 = np.array([0.8, -0.4, 0.1, 1.0], np.float32)
+        a1 = np.array([0.3, 0.5, 0.2, 1.0], np.float32)
+        st = O.pack_isaac_states(256, 3 + v["idx"])
+        st2 = st.copy()
+        O.ref_eval_grid(v["idx"], pts, 0.75, p, a0, a1, st2)
+        if not np.array_equal(st, st2):
+            wrong.append(v["name"])
+    assert not wrong, wrong
+    assert 60 <= len(draws) <= 90
