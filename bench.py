@@ -537,7 +537,7 @@ def bench_denoise(args, ws, rank, local, dist):
     n_tr = n_gen - n_ho
     xtr, ttr, xho, tho = xs[:n_tr], ts[:n_tr], xs[n_tr:], ts[n_tr:]
     per = 200
-    batch, crop = 8, 128
+    batch, crop = args.dn_batch, args.dn_crop
     in_ch = args.dn_input
     net, _, _ = DN.train(xtr, ttr, steps=per * args.warmup, batch=batch, crop=crop, seed=1, in_ch=in_ch)
     params = net.params()
@@ -569,7 +569,7 @@ def bench_denoise(args, ws, rank, local, dist):
     rng = np.random.default_rng(3)
     hnet = DN.UNet(batch, crop, crop, net.params(), in_ch=in_ch)
     hnet.capture()
-    n_e2e = per
+    n_e2e = max(20, per * 8 * 128 * 128 // (batch * crop * crop))  # host-assembled batches: ~200 of 8 x 128^2
     hx = np.empty((batch, DN.IN_CH + DN.OUT_CH, crop, crop), np.float32)
     ht = np.empty((batch, 3, crop, crop), np.float32)
     torch.cuda.synchronize()
@@ -856,6 +856,8 @@ def main():
     ap.add_argument("--dn-genomes", type=int, default=136,
                     help="denoise: seeded genomes rendered for the dataset (the last 8 held out)")
     ap.add_argument("--dn-size", type=int, default=384, help="denoise: canvas side of the dataset renders")
+    ap.add_argument("--dn-batch", type=int, default=8, help="denoise: crops per Adam step")
+    ap.add_argument("--dn-crop", type=int, default=128, help="denoise: crop side (a multiple of 16)")
     ap.add_argument("--dn-input", type=int, default=8, choices=[8, 11],
                     help="denoise: network input channels: the 8 features, or 11 with the noisy RGB")
     ap.add_argument("--samples", type=int, default=0,
