@@ -545,7 +545,7 @@ def bench_denoise(args, ws, rank, local, dist):
     _barrier(dist)
     clocks = Clocks(local) if rank == 0 else None
     net, losses, ms = DN.train(xtr, ttr, steps=per * args.steps, batch=batch, crop=crop, seed=2,
-                               params=params, in_ch=in_ch)
+                               params=params, in_ch=in_ch, lr_end=args.dn_lr_end)
     launches = net.launches
     clk = clocks.stop() if clocks else None
     t_max = _max_over_ranks(ms, dist, local)
@@ -606,7 +606,8 @@ def bench_denoise(args, ws, rank, local, dist):
                    "params": DN.param_count(in_ch=in_ch), "canvas": [size, size], "spp_input": 25, "spp_target": 2000,
                    "input_channels": in_ch, "train_genomes": n_tr, "held_out_genomes": n_ho,
                    "batch": batch, "crop": crop,
-                   "adam_steps_per_step": per, "l2": "inputs resident; working set < L2 per layer",
+                   "adam_steps_per_step": per, "lr": [1e-3, args.dn_lr_end if args.dn_lr_end is not None else 1e-3],
+                   "l2": "inputs resident; working set < L2 per layer",
                    "parallelism": f"replicas x{ws}"},
         "quality": {"held_out_psnr_input_db": p_noisy, "held_out_psnr_denoised_db": p_dn,
                     "held_out_ssim_input": ssim_in, "held_out_ssim_denoised": ssim_dn,
@@ -857,6 +858,8 @@ def main():
                     help="denoise: seeded genomes rendered for the dataset (the last 8 held out)")
     ap.add_argument("--dn-size", type=int, default=384, help="denoise: canvas side of the dataset renders")
     ap.add_argument("--dn-batch", type=int, default=8, help="denoise: crops per Adam step")
+    ap.add_argument("--dn-lr-end", type=float, default=None,
+                    help="denoise: learning rate the timed steps fall to linearly (from 1e-3)")
     ap.add_argument("--dn-crop", type=int, default=128, help="denoise: crop side (a multiple of 16)")
     ap.add_argument("--dn-input", type=int, default=8, choices=[8, 11],
                     help="denoise: network input channels: the 8 features, or 11 with the noisy RGB")

@@ -420,9 +420,10 @@ def make_dataset(genomes, spp_in: float = 25.0, spp_target: float = 2000.0, seed
 
 
 def train(xs, ts, steps: int = 300, batch: int = 8, crop: int = 128, lr: float = 1e-3, seed: int = 0,
-          chans=CHANS, params=None, in_ch: int = IN_CH):
-    """Adam on random crops of (xs, ts), all on the device.  Returns (net,
-    losses, device ms of the training steps)."""
+          chans=CHANS, params=None, in_ch: int = IN_CH, lr_end: float | None = None):
+    """Adam on random crops of (xs, ts), all on the device; the learning
+    rate falls linearly from lr to lr_end over the steps when lr_end is
+    given.  Returns (net, losses, device ms of the training steps)."""
     import torch
 
     rng = np.random.default_rng(seed)
@@ -444,7 +445,7 @@ def train(xs, ts, steps: int = 300, batch: int = 8, crop: int = 128, lr: float =
             net.x[j].copy_(X[idx[j], :, ys[j]:ys[j] + crop, xo[j]:xo[j] + crop])
             net.tgt[j].copy_(T[idx[j], :, ys[j]:ys[j] + crop, xo[j]:xo[j] + crop])
         net.replay()
-        net.step(lr=lr)
+        net.step(lr=lr if lr_end is None else lr + (lr_end - lr) * s / max(1, steps - 1))
         if s % 25 == 0 or s == steps - 1:
             losses.append((s, net.read_loss()))
     e1.record()
