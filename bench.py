@@ -518,10 +518,12 @@ def bench_reference(args, ws, rank, local, dist):
 
 
 def bench_denoise(args, ws, rank, local, dist):
-    """Learned denoiser: a step = 200 Adam steps on batches of 8 random
-    128x128 crops from 64 training genomes' (25 spp features, 2000 spp
-    target) renders at 256x256; afterwards the 8 held-out genomes are
-    denoised and scored (PSNR against their 2000-spp renders)."""
+    """Learned denoiser: a step = 200 Adam steps on batches of --dn-batch
+    random --dn-crop square crops (default 32 x 256^2) from the training
+    genomes' renders (25 spp features, 2000 spp target; --dn-genomes
+    genomes at --dn-size, default 136 at 384^2, the last 8 held out);
+    afterwards the held-out genomes are denoised and scored (PSNR and SSIM
+    against their 2000-spp renders, and the plain spp that matches)."""
     import time as _t
 
     import torch
@@ -857,10 +859,10 @@ def main():
     ap.add_argument("--dn-genomes", type=int, default=136,
                     help="denoise: seeded genomes rendered for the dataset (the last 8 held out)")
     ap.add_argument("--dn-size", type=int, default=384, help="denoise: canvas side of the dataset renders")
-    ap.add_argument("--dn-batch", type=int, default=8, help="denoise: crops per Adam step")
+    ap.add_argument("--dn-batch", type=int, default=32, help="denoise: crops per Adam step")
     ap.add_argument("--dn-lr-end", type=float, default=None,
                     help="denoise: learning rate the timed steps fall to linearly (from 1e-3)")
-    ap.add_argument("--dn-crop", type=int, default=128, help="denoise: crop side (a multiple of 16)")
+    ap.add_argument("--dn-crop", type=int, default=256, help="denoise: crop side (a multiple of 16)")
     ap.add_argument("--dn-input", type=int, default=8, choices=[8, 11],
                     help="denoise: network input channels: the 8 features, or 11 with the noisy RGB")
     ap.add_argument("--samples", type=int, default=0,

@@ -366,7 +366,7 @@ int pyr3_dn_conv3x3_wgrad(const float *in, int64_t in_ns, int32_t ci, const floa
                           void *stream);
 /* pyr3_dn_conv3x3_wgrad on the tensor cores (tcgen05): per tap a GEMM over
  * pixel positions with input and output gradient rounded to bf16 and f32
- * accumulation; co, ci <= 128 and n <= 32 (PYR3_E_INVALID otherwise), the
+ * accumulation; co, ci <= 128 and n <= 128 (PYR3_E_INVALID otherwise), the
  * same scratch. */
 int pyr3_dn_conv3x3_wgrad_bf16(const float *in, int64_t in_ns, int32_t ci, const float *dout,
                                int64_t dout_ns, int32_t co, int32_t n, int32_t h, int32_t w,

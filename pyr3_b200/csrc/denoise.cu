@@ -15,7 +15,7 @@ namespace {
 constexpr int TS = 16;    // output tile edge
 constexpr int CO_B = 8;   // output channels per block
 constexpr int CI_B = 4;   // input channels staged per step
-constexpr int kWgChunks = 32;  // pixel chunks of the weight gradient
+constexpr int kWgChunks = 128;  // pixel chunks of the weight gradient (partials added in a fixed order)
 
 __global__ void __launch_bounds__(256)
 k_conv3x3(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __restrict__ out,
@@ -265,17 +265,19 @@ unsigned blocks_for(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / 
 // Implicit GEMM without im2col.  Index the zero-padded input by position
 // q = (y + 1) * P + (x + 1), P = W + 2: output q reads input q + d for tap
 // (ky, kx), d = (ky - 1) * P + (kx - 1) -- the same shift for every pixel.
-// A CTA owns 128 consecutive output positions (M = 128; positions in the
-// padding columns are computed and dropped) and stages the padded input
-// rows it needs, R = 128 + 2 (P + 1), once: plane g holds channels 8g..8g+7
+// A CTA owns T tiles of 128 consecutive output positions (M = 128 each;
+// positions in the padding columns are computed and dropped; T <= 4, one
+// TMEM accumulator per tile) and stages the padded input rows they need,
+// R = 128 T + 2 (P + 1), once -- the tap window of the tiles' rows above and
+// below is shared by all T tiles: plane g holds channels 8g..8g+7
 // as one 16-byte bf16 row per position, so the operand of tap t and K step
 // s (channels 16s..16s+15) is planes 2s and 2s+1 read from row P + 1 + d_t:
 // a no-swizzle K-major descriptor with contiguous rows (SBO = 16 B x 8) and
 // the next plane at LBO = 16 R bytes.  Per tap the weights (all output
 // channels, N = NP padded to 16) are staged in the usual canonical layout,
-// one thread issues the tap's MMAs into the TMEM accumulator and commits
-// them to an mbarrier that every thread waits on (bounded) before the
-// weights are refilled.  Each warp reads its 32 rows back (tcgen05.ld),
+// once for all T tiles; one thread issues the tap's MMAs of every tile into
+// its TMEM accumulator and commits them to an mbarrier that every thread
+// waits on (bounded) before the weights are refilled.  Each warp reads its 32 rows back (tcgen05.ld),
 // adds the bias, applies ReLU and stores the interior pixels in f32.
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;
 constexpr int TC_MAX_SMEM = 200 * 1024;
@@ -293,9 +295,9 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// Dynamic shared memory of the tensor-core convolution (bytes).
-__host__ __device__ inline size_t tc_smem_bytes(int ci, int w, int np) {
-  const size_t R = 128 + 2 * (size_t)(w + 3);
+// Dynamic shared memory of the tensor-core convolution (bytes), T tiles.
+__host__ __device__ inline size_t tc_smem_bytes(int ci, int w, int np, int T) {
+  const size_t R = 128 * (size_t)T + 2 * (size_t)(w + 3);
   const size_t G = 2 * (size_t)((ci + 15) / 16);
   return G * R * 16 + (G / 2) * (size_t)np * 32;
 }
@@ -303,17 +305,21 @@ __host__ __device__ inline size_t tc_smem_bytes(int ci, int w, int np) {
 template <int NP>
 __global__ void __launch_bounds__(128)
 k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __restrict__ out, int64_t out_ns,
-             int co_n, int H, int W, const float* __restrict__ wt, const float* __restrict__ bias, int relu) {
+             int co_n, int H, int W, const float* __restrict__ wt, const float* __restrict__ bias, int relu,
+             int T) {
   constexpr uint32_t NCOL = NP <= 32 ? 32 : (NP <= 64 ? 64 : 128);
+  // TMEM columns: one NCOL accumulator per tile, allocated as a power of two.
+  const uint32_t ncols = (uint32_t)T * NCOL <= 32u ? 32u : ((uint32_t)T * NCOL <= 64u ? 64u :
+                         ((uint32_t)T * NCOL <= 128u ? 128u : ((uint32_t)T * NCOL <= 256u ? 256u : 512u)));
   extern __shared__ __align__(1024) unsigned char smem[];
-  const int P = W + 2, R = 128 + 2 * (P + 1), G = 2 * ((ci_n + 15) / 16), S = G / 2;
+  const int P = W + 2, R = 128 * T + 2 * (P + 1), G = 2 * ((ci_n + 15) / 16), S = G / 2;
   uint4* sa = reinterpret_cast<uint4*>(smem);  // G planes x R rows of 16 B
   uint4* sb = sa + (size_t)G * R;               // S K steps x (NP / 8) x 2 core matrices x 8 rows
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_base;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int n = blockIdx.y;
-  const int q0 = P + 1 + blockIdx.x * 128;  // first output position of the tile
+  const int q0 = P + 1 + blockIdx.x * 128 * T;  // first output position of the CTA's first tile
   const int qa = q0 - (P + 1);              // position of staged row 0
   const int64_t hw = (int64_t)H * W;
   const float* inn = in + n * in_ns;
@@ -323,7 +329,7 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base)),
-                 "r"(NCOL) : "memory");
+                 "r"(ncols) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   // padded input rows: plane g, row r = position qa + r, 8 channels as bf16
@@ -365,13 +371,15 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
     if (t == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int row0 = (P + 1) + (tap / 3 - 1) * P + (tap % 3 - 1);
-      for (int s = 0; s < S; ++s) {
-        const uint64_t da = umma_desc(smem_addr(sa + (size_t)(2 * s) * R + row0), lbo_a, 128u);
-        const uint64_t db = umma_desc(smem_addr(sb + (size_t)s * NP * 2), 128u, 256u);
-        const uint32_t acc = (tap > 0 || s > 0) ? 1u : 0u;
-        asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-                     ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+      for (int m = 0; m < T; ++m) {  // tile m: rows 128 m.. of the window, accumulator columns m NCOL..
+        for (int s = 0; s < S; ++s) {
+          const uint64_t da = umma_desc(smem_addr(sa + (size_t)(2 * s) * R + row0 + 128 * m), lbo_a, 128u);
+          const uint64_t db = umma_desc(smem_addr(sb + (size_t)s * NP * 2), 128u, 256u);
+          const uint32_t acc = (tap > 0 || s > 0) ? 1u : 0u;
+          asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                       " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                       ::"r"(tmem + (uint32_t)m * NCOL), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+        }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                    ::"r"(smem_addr(&bar)) : "memory");
@@ -382,24 +390,27 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
                    : "=r"(done) : "r"(smem_addr(&bar)), "r"((uint32_t)(tap & 1)) : "memory");
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
-  // epilogue: TMEM row i = output position q0 + i
-  const int q = q0 + warp * 32 + lane, oy = q / P - 1, ox = q % P - 1;
-  const bool inside = oy >= 0 && oy < H && ox >= 0 && ox < W;
+  // epilogue: TMEM row i of accumulator m = output position q0 + 128 m + i
 #pragma unroll 1
-  for (int c0 = 0; c0 < NP; c0 += 8) {
-    uint32_t v[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-                 : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    if (inside) {
+  for (int m = 0; m < T; ++m) {
+    const int q = q0 + 128 * m + warp * 32 + lane, oy = q / P - 1, ox = q % P - 1;
+    const bool inside = oy >= 0 && oy < H && ox >= 0 && ox < W;
+#pragma unroll 1
+    for (int c0 = 0; c0 < NP; c0 += 8) {
+      uint32_t v[8];
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                   : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                   : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(m * NCOL + c0)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (inside) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int co = c0 + j;
-        if (co < co_n) {
-          float x = __uint_as_float(v[j]) + (bias ? bias[co] : 0.0f);
-          if (relu) x = fmaxf(x, 0.0f);
-          out[n * out_ns + co * hw + (int64_t)oy * W + ox] = x;
+        for (int j = 0; j < 8; ++j) {
+          const int co = c0 + j;
+          if (co < co_n) {
+            float x = __uint_as_float(v[j]) + (bias ? bias[co] : 0.0f);
+            if (relu) x = fmaxf(x, 0.0f);
+            out[n * out_ns + co * hw + (int64_t)oy * W + ox] = x;
+          }
         }
       }
     }
@@ -407,7 +418,7 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
 // ---- weight gradient on the tensor cores
@@ -456,17 +467,28 @@ k_wgrad_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, const float* _
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NP >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  // A rows co_n..127 (output channels past the layer's) are zero for every step.
+  for (int idx = co_n * (WT_KC / 8) + t; idx < 128 * (WT_KC / 8); idx += 128) {
+    const int co = idx >> 3, g = idx & 7, s = g >> 1, h = g & 1;
+    sa[(s * 32 + (co >> 3) * 2 + h) * 8 + (co & 7)] = make_uint4(0u, 0u, 0u, 0u);
+  }
   int phase = 0;
   for (int qs = q_begin; qs < q_end; qs += WT_KC, ++phase) {
-    // A rows: output channel co (128 rows), 8 positions per 16-byte row
-    for (int idx = t; idx < 128 * (WT_KC / 8); idx += 128) {
+    // A rows: output channel co (128 rows), 8 positions per 16-byte row.
+    // Rows past co_n stay zero (written once, below); the padded-grid
+    // coordinates of a group's first position are divided out once and
+    // stepped along the row.
+    for (int idx = t; idx < co_n * (WT_KC / 8); idx += 128) {
       const int co = idx >> 3, g = idx & 7;
+      const int q0 = qs + g * 8;
+      int yy = q0 / P, xx = q0 - yy * P;
+      const float* src = dn + co * hw;
       float v[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const int q = qs + g * 8 + j, y = q / P - 1, x = q % P - 1;
-        v[j] = (co < co_n && q < q_end && y >= 0 && y < H && x >= 0 && x < W) ? dn[co * hw + (int64_t)y * W + x]
-                                                                             : 0.0f;
+        v[j] = (q0 + j < q_end && yy >= 1 && yy <= H && xx >= 1 && xx <= W) ? src[(int64_t)(yy - 1) * W + (xx - 1)]
+                                                                          : 0.0f;
+        if (++xx == P) { xx = 0; ++yy; }
       }
       const int s = g >> 1, h = g & 1;
       sa[(s * 32 + (co >> 3) * 2 + h) * 8 + (co & 7)] =
@@ -475,12 +497,16 @@ k_wgrad_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, const float* _
     // B rows: input channel ci, the positions shifted by the tap
     for (int idx = t; idx < NP * (WT_KC / 8); idx += 128) {
       const int ci = idx >> 3, g = idx & 7;
+      const int q0 = qs + g * 8, qi0 = q0 + d;
+      int yy = qi0 / P, xx = qi0 - yy * P;
+      const float* src = ip + ci * hw;
       float v[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const int q = qs + g * 8 + j, qi = q + d, y = qi / P - 1, x = qi % P - 1;
-        v[j] = (ci < ci_n && q < q_end && y >= 0 && y < H && x >= 0 && x < W) ? ip[ci * hw + (int64_t)y * W + x]
-                                                                             : 0.0f;
+        v[j] = (ci < ci_n && q0 + j < q_end && yy >= 1 && yy <= H && xx >= 1 && xx <= W)
+                   ? src[(int64_t)(yy - 1) * W + (xx - 1)]
+                   : 0.0f;
+        if (++xx == P) { xx = 0; ++yy; }
       }
       const int s = g >> 1, h = g & 1;
       sb[(s * (NP / 4) + (ci >> 3) * 2 + h) * 8 + (ci & 7)] =
@@ -605,7 +631,16 @@ cudaError_t dn_conv3x3_wgrad_bf16(const float* in, int64_t in_ns, int ci, const 
 template <int NP>
 cudaError_t launch_tc(const float* in, int64_t in_ns, int ci, float* out, int64_t out_ns, int co, int n, int h,
                       int w, const float* weight, const float* bias, bool relu, cudaStream_t s) {
-  const size_t smem = tc_smem_bytes(ci, w, NP);
+  // Tiles per CTA: up to 4 (512 TMEM columns at NP = 128) while the launch
+  // keeps at least four CTAs per SM (148 SMs); fewer where the staged
+  // window would not fit.  One tile per CTA for small launches, whose
+  // parallelism matters more than the shared window.
+  const int P = w + 2;
+  const int64_t span = (int64_t)(h - 1) * P + w;  // output positions from the first to the last pixel
+  const int64_t tiles = (span + 127) / 128;
+  int T = (int)std::max<int64_t>(1, std::min<int64_t>({4, tiles, tiles * n / (4 * 148)}));
+  while (T > 1 && tc_smem_bytes(ci, w, NP, T) > (size_t)TC_MAX_SMEM) --T;
+  const size_t smem = tc_smem_bytes(ci, w, NP, T);
   if (smem > (size_t)TC_MAX_SMEM) return cudaErrorInvalidValue;
   static bool attr = false;  // per instantiation; the same limit on every device
   if (!attr) {
@@ -613,10 +648,8 @@ cudaError_t launch_tc(const float* in, int64_t in_ns, int ci, float* out, int64_
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int P = w + 2;
-  const int64_t span = (int64_t)(h - 1) * P + w;  // output positions from the first to the last pixel
-  const dim3 grid((unsigned)((span + 127) / 128), n);
-  k_conv3x3_tc<NP><<<grid, 128, smem, s>>>(in, in_ns, ci, out, out_ns, co, h, w, weight, bias, relu ? 1 : 0);
+  const dim3 grid((unsigned)((tiles + T - 1) / T), n);
+  k_conv3x3_tc<NP><<<grid, 128, smem, s>>>(in, in_ns, ci, out, out_ns, co, h, w, weight, bias, relu ? 1 : 0, T);
   return cudaGetLastError();
 }
 

@@ -227,6 +227,28 @@ def test_cuda_layers_match_oracle():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n,ci,co,h,w", [(1, 40, 16, 48, 130), (3, 8, 96, 17, 256), (2, 88, 40, 8, 8)])
+def test_tensor_core_convolution_tiles_match_oracle(n, ci, co, h, w):
+    """The tcgen05 convolution with several 128-position tiles per CTA
+    sharing one staged window (wide rows: 130 and 256 columns; a tail CTA
+    whose last tiles lie past the image) and with one tile (an 8 x 8
+    level): the oracle on bf16-rounded operands, f32 sums."""
+    from pyr3_b200 import _lib
+
+    rng = np.random.default_rng(ci + co + w)
+    x = rng.normal(size=(n, ci, h, w))
+    wt = rng.normal(size=(co, ci, 3, 3)) * 0.2
+    b = rng.normal(size=co)
+    xd, wd, bd = _dev(x), _dev(wt), _dev(b)
+    y = torch.zeros((n, co, h, w), device="cuda")
+    _lib.check(_lib.lib().pyr3_dn_conv3x3_bf16(_p(xd), ci * h * w, ci, _p(y), co * h * w, co, n, h, w,
+                                               C.c_void_p(wd.data_ptr()), C.c_void_p(bd.data_ptr()), 1, None))
+    torch.cuda.synchronize()
+    want = D.conv3x3(_bf16(x), _bf16(wt), b.astype(np.float32).astype(np.float64), relu=True)
+    _close(y, want, rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("in_ch", [8, 11])
 def test_cuda_unet_forward_backward_matches_oracle(in_ch):
     """The whole U-Net's output and parameter gradient against the numpy
