@@ -531,7 +531,7 @@ def bench_denoise(args, ws, rank, local, dist):
     from pyr3_b200 import denoise as DN
     from pyr3_b200 import workloads
 
-    n_gen, size, n_ho = args.dn_genomes, args.dn_size, 8
+    n_gen, size, n_ho = args.dn_genomes, args.dn_size, args.dn_held_out
     gs = workloads.denoise_set(seed=5 + 1000 * rank, n=n_gen, size=size)
     t0 = _t.perf_counter()
     xs, ts = DN.make_dataset(gs)
@@ -857,8 +857,9 @@ def main():
     ap.add_argument("--kernel", default="auto", choices=["auto", "barrier", "queue", "wave"],
                     help="chaos kernel (auto: the autotuner's choice)")
     ap.add_argument("--dn-genomes", type=int, default=136,
-                    help="denoise: seeded genomes rendered for the dataset (the last 8 held out)")
+                    help="denoise: seeded genomes rendered for the dataset (the last --dn-held-out held out)")
     ap.add_argument("--dn-size", type=int, default=384, help="denoise: canvas side of the dataset renders")
+    ap.add_argument("--dn-held-out", type=int, default=8, help="denoise: genomes held out for scoring")
     ap.add_argument("--dn-batch", type=int, default=32, help="denoise: crops per Adam step")
     ap.add_argument("--dn-lr-end", type=float, default=None,
                     help="denoise: learning rate the timed steps fall to linearly (from 1e-3)")
