@@ -182,6 +182,14 @@ int device_sms(int dev) {
   return g_num_sms > 0 ? g_num_sms : 148;
 }
 
+int g_l2_bytes = 0;
+
+// L2 size in bytes (126 MiB on B200).
+uint64_t device_l2(int dev) {
+  if (g_l2_bytes == 0) cudaDeviceGetAttribute(&g_l2_bytes, cudaDevAttrL2CacheSize, dev);
+  return g_l2_bytes > 0 ? (uint64_t)g_l2_bytes : (126ull << 20);
+}
+
 }  // namespace
 
 struct pyr3_renderer {
@@ -472,23 +480,27 @@ int launch_chaos(pyr3_renderer* r, const pyr3::ChaosModule& m, bool queue, Chaos
   return PYR3_OK;
 }
 
-// Walkers of a wave launch of `total` samples: about 2,000 iterations each,
-// so the 200-iteration burn-in stays near 10 %, yet enough that every
-// launch fills the GPU twice over; at most 2^20, whose state (42 u32 per
-// walker and region, two buffers) stays within a few GB.
+// Most walkers one wave launch takes (a caller's explicit count): their
+// state (49 u32 per walker and region, two buffers) stays within a few GB.
 constexpr uint64_t kWaveMaxWalkers = 1ull << 21;
 // Walkers of a wave launch: total / 2000 for large launches (2,000
-// iterations each), at least enough to fill the GPU twice over (two
-// populations) -- but a small launch takes only sqrt(1200 * total), since
-// every walker also runs the 200-iteration burn-in: measured on B200 at 2e6,
-// 9.4e6 and 3.4e7 samples, that is within 5 % of the best walker count,
-// where the fill alone was 7-38 % slower.
+// iterations each), but no more than the walkers whose state fills half of
+// L2, so a walker's record, written at the end of one iteration, is still
+// in L2 when the next launch of its population copies it in (the copy then
+// drops the lines, see chaos_wave_kernel); at least enough to fill the GPU
+// twice over (two populations) -- but a small launch takes only
+// sqrt(1200 * total), since every walker also runs the 200-iteration
+// burn-in: measured on B200 at 2e6, 9.4e6 and 3.4e7 samples, that is within
+// 5 % of the best walker count, where the fill alone was 7-38 % slower.
+// On the headline genome (1.04e9 samples) pools of 227 K-346 K walkers run
+// within 2 % of each other and 15 % faster than 518 K, whose state spills
+// to HBM.
 uint64_t wave_walkers(pyr3_renderer* r, const pyr3::ChaosModule& m, uint64_t total) {
-  const uint64_t fill =
-      (uint64_t)device_sms(r->device) * (uint64_t)m.wave_blocks_per_sm * pyr3::kWaveBlock * 2;
+  const uint64_t wb2 = 2ull * pyr3::kWaveBlock;
+  const uint64_t fill = (uint64_t)device_sms(r->device) * (uint64_t)m.wave_blocks_per_sm * wb2;
+  const uint64_t l2 = std::max<uint64_t>(fill, device_l2(r->device) / 2 / (pyr3::kWaveFields * 4) / wb2 * wb2);
   const uint64_t small = (uint64_t)std::sqrt(1200.0 * (double)total);
-  const uint64_t want =
-      std::min<uint64_t>(1ull << 20, std::max<uint64_t>(std::min<uint64_t>(fill, small), total / 2000));
+  const uint64_t want = std::max<uint64_t>(std::min<uint64_t>(fill, small), std::min<uint64_t>(l2, total / 2000));
   return std::max<uint64_t>(1, std::min<uint64_t>(want, total));
 }
 

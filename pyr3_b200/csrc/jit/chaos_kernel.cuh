@@ -905,6 +905,10 @@ chaos_queue_kernel(const __grid_constant__ ChaosArgs A) {
 // sorts its walkers by their next xform in shared memory, reserves room in
 // the next buffer's regions with one atomicAdd per xform, and writes the
 // walkers out in sorted order (coalesced).  No block ever waits on another.
+// The host sizes the pool so both populations' records fit in half of L2;
+// records are written with an evict-last policy and dropped from L2 once
+// copied in, so between launches they need not touch HBM, which is left to
+// the histogram's atomics.
 //
 // State: st[2][NXF][WF][cap] u32 (two buffers, field-major so a chunk's
 // field is one contiguous 1 KB line) -- fields 0..42 the ISAAC state in the
@@ -971,6 +975,10 @@ VDEV void mbar_expect_tx(u64* bar, u32 bytes) {
 VDEV void bulk_g2s(void* dst, const void* src, u32 bytes, u64* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
                ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// 4-byte store cached in L2 only (st.global.cg) under L2 cache policy pol.
+VDEV void st_keep(u32* dst, u32 v, u64 pol) {
+  asm volatile("st.global.cg.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(dst), "r"(v), "l"(pol) : "memory");
 }
 // Wait for phase 0 of the barrier; false if WAVE_WAIT_LIMIT polls pass.
 VDEV bool mbar_wait0(u64* bar) {
@@ -1083,6 +1091,19 @@ chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ W
       mbar_wait0(&wbar);
       return;
     }
+    // The chunk's source lines are dead once copied: this launch reads each
+    // chunk once, and the buffer is next read after the following launch has
+    // rewritten it.  Dropping them from L2 (no write-back) keeps the records
+    // of both populations L2-resident between launches.  Every field's chunk
+    // is 1 KB aligned in the host layout; lines are dropped only where the
+    // 128-byte alignment the instruction needs holds.
+    if (((reinterpret_cast<unsigned long long>(wave_field(W, W.rd_buf, k, 0) + pos0) | (W.cap * 4ull)) &
+         127ull) == 0ull) {
+      for (u32 q = t; q < (u32)WF * 8u; q += WB) {
+        const u32* src = wave_field(W, W.rd_buf, k, q >> 3) + pos0 + (q & 7u) * 32u;
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(src) : "memory");
+      }
+    }
     if (pos < swork[2]) {
       p = f2(__uint_as_float(sfs[t]), __uint_as_float(sfs[WB + t]));
       z = __uint_as_float(sfs[2 * WB + t]);
@@ -1154,11 +1175,14 @@ chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ W
   __syncthreads();
   if (t < soff[NXF]) {
     const u32 src = sperm[t], kk = skey[t], g = sdst[t];
+    // Written with an evict-last L2 policy: the next launch of this
+    // population reads the records back.
+    u64 pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
 #pragma unroll 4
-    for (u32 f = 0; f < (u32)WRNG; ++f)
-      __stcg(wave_field(W, W.wr_buf, kk, f) + g, srng[f * WB + src]);
+    for (u32 f = 0; f < (u32)WRNG; ++f) st_keep(wave_field(W, W.wr_buf, kk, f) + g, srng[f * WB + src], pol);
 #pragma unroll
-    for (u32 f = 0; f < 6u; ++f) __stcg(wave_field(W, W.wr_buf, kk, WRNG + f) + g, sfs[f * WB + src]);
+    for (u32 f = 0; f < 6u; ++f) st_keep(wave_field(W, W.wr_buf, kk, WRNG + f) + g, sfs[f * WB + src], pol);
   }
 }
 #endif  // WAVE

@@ -828,6 +828,35 @@ def test_wave_kernel_pool_split():
     r.destroy()
 
 
+def test_wave_kernel_pool_fits_half_of_l2():
+    """A default wave launch of 10^9 samples takes the walkers whose records
+    (196 B each) fill half of L2 -- 336,896 on B200, ~2,968 iterations each,
+    where 2,000-iteration walkers would be 500,000 -- so the launch count (a
+    seeding launch, one per iteration, a last launch, for each of the two
+    populations) shows more than 2,500 iterations.  Every sample is counted
+    once and the count channel holds 255 per in-canvas splat, with the
+    records written under an evict-last policy and dropped from L2 after
+    each copy.  The 1280x720 canvas keeps every cell far below 2^32 (on a
+    small canvas the hot cells of 10^9 samples saturate, and the count
+    channel no longer sums to 255 per splat)."""
+    g = _linear_genome(n=5, seed=11, blowup=False)
+    g.scale = 1280 / 4
+    r = R.create_renderer(1280, 720, 1)
+    r.reset(g)
+    total = 1_000_000_000
+    r.iterate(g, seed=4, walkers=1000, iters_per_walker=total // 1000, kernel="wave")
+    launches = r.last_iterate_launches()
+    s, n_in = r.counters()
+    assert s == total
+    hist, _, _ = r.read_histogram()
+    assert int(hist.max()) < 0xFFFFFFFF
+    assert int(hist.reshape(-1, 4)[:, 3].astype(np.uint64).sum()) == 255 * n_in
+    assert n_in > 0
+    iters = launches // 2 - 202
+    assert 2500 < iters < 4000, launches
+    r.destroy()
+
+
 def test_queue_kernel_refills_walker_slots():
     """More walkers than the resident slots (exact-walkers mode), so slots
     are refilled as walkers finish: every walker runs exactly its

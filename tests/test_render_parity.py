@@ -16,7 +16,7 @@ variations, so the comparison is statistical, on two measures:
 The genomes are the benchmark's own (pyr3_b200/workloads.py) on reduced
 canvases at the benchmark's samples per pixel: the headline genome (12
 catalog xforms, post affines, final xform) through the wave kernel at the
-bench's ~2,000 iterations per walker and at the short-trajectory pool of a
+bench's ~3,077 iterations per walker and at the short-trajectory pool of a
 small launch; the motion_4k genome (direct-colour variations, 8 box-
 filtered sub-frames, density estimation 15/0/0.6 at oversample 2, radius
 31); and eight batch_256 genomes through one batch."""
@@ -67,16 +67,21 @@ def _check(name, g, dev_hist, dev_img, ref1, ref2, W, H, os_, samples):
     return l1, floor, p_dev, p_floor
 
 
-@pytest.mark.parametrize("pool,W,H,spp", [("bench_2000_iters", 480, 270, 500),
+# Iterations per walker of the bench's headline launch: 1.0368e9 samples on
+# 336,896 walkers (the wave pool whose records fill half of L2).
+BENCH_ITERS = 3077
+
+
+@pytest.mark.parametrize("pool,W,H,spp", [("bench_iters", 480, 270, 500),
                                           ("short_trajectories", 480, 270, 500),
-                                          ("bench_2000_iters", 192, 108, 6000)])
+                                          ("bench_iters", 192, 108, 6000)])
 def test_headline_genome_matches_reference(pool, W, H, spp):
     """The headline genome (1920x1080 os 2, 500 spp, 12 catalog xforms +
     final) on reduced os-2 canvases through the wave kernel, against the
     reference's computeDispatch split (1024 walkers):
 
-    * 480x270 at the bench's 500 spp (6.48e7 samples), with walkers of 2,000
-      iterations (the bench's iterations per walker: 518,400 x 2,000 at full
+    * 480x270 at the bench's 500 spp (6.48e7 samples), with walkers of 3,077
+      iterations (the bench's iterations per walker: 336,896 walkers at full
       size), and with the small-launch pool (~279k walkers of ~232
       iterations, where the 200-iteration burn-in weighs most).  At 500 spp
       two reference seeds are themselves only ~32.6 dB apart, so the image
@@ -85,8 +90,8 @@ def test_headline_genome_matches_reference(pool, W, H, spp):
       reference floor is above 40 dB: the device render is at least 40 dB
       from the reference.
 
-    With 2,000-iteration walkers the device draws samples // 2000 x 2000
-    samples (at most 1,999 fewer than the reference), and each image is
+    With 3,077-iteration walkers the device draws samples // 3077 x 3077
+    samples (at most 3,076 fewer than the reference), and each image is
     presented with its own sample count."""
     g = workloads.headline_1080p()
     os_ = 2
@@ -96,9 +101,9 @@ def test_headline_genome_matches_reference(pool, W, H, spp):
     ref2 = ref_chaos(g, W * os_, H * os_, iters, walkers, seed=31, oversample=os_)
     r = R.create_renderer(W, H, os_)
     r.reset(g)
-    if pool == "bench_2000_iters":
-        dev_samples = samples // 2000 * 2000
-        r.iterate(g, seed=77, walkers=dev_samples // 2000, iters_per_walker=2000, exact_walkers=True,
+    if pool == "bench_iters":
+        dev_samples = samples // BENCH_ITERS * BENCH_ITERS
+        r.iterate(g, seed=77, walkers=dev_samples // BENCH_ITERS, iters_per_walker=BENCH_ITERS, exact_walkers=True,
                   kernel="wave")
     else:
         dev_samples = samples
