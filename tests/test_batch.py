@@ -2,8 +2,10 @@
 the same genome rendered alone through the per-genome path -- statistically,
 since walker counts and seeds differ -- and gets exactly its samples.  Two
 genomes of the batch share a structure, so each needs its own module
-instance; the last genome is large enough (>= 2^24 samples) to run beside
-the graph through the per-genome path, on a structure the graph also uses."""
+instance.  The last three genomes are large enough (>= 2^24 samples) to run
+beside the graph through the per-genome path, one after another; two of
+them share a structure with each other and with graph genomes (module
+instance 0 beside the graph's instances)."""
 import copy
 
 import numpy as np
@@ -27,14 +29,19 @@ def _genomes():
                                         zip((x.a, x.b, x.c, x.d, x.e, x.f), rng.uniform(-0.1, 0.1, 6)))
     b, _ = workloads.motion_4k()
     big = copy.deepcopy(a2)
-    gs = [a, a2, b, big]
+    big2 = copy.deepcopy(b)
+    big3 = copy.deepcopy(a)
+    for x in big3.xforms:
+        x.c, x.f = x.c + 0.05, x.f - 0.05
+    gs = [a, a2, b, big, big2, big3]
     for g in gs:
         g.size = (W, H)
         g.oversample = 1
         g.density = None
         g.scale = W / 4
         g.quality = 640.0  # 1.2e7 samples each: in the graph
-    big.quality = 3600.0  # 6.9e7 samples: beside the graph
+    for g in (big, big2, big3):
+        g.quality = 3600.0  # 6.9e7 samples: beside the graph
     return gs
 
 
