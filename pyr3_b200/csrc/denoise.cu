@@ -273,12 +273,13 @@ unsigned blocks_for(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / 
 // as one 16-byte bf16 row per position, so the operand of tap t and K step
 // s (channels 16s..16s+15) is planes 2s and 2s+1 read from row P + 1 + d_t:
 // a no-swizzle K-major descriptor with contiguous rows (SBO = 16 B x 8) and
-// the next plane at LBO = 16 R bytes.  Per tap the weights (all output
-// channels, N = NP padded to 16) are staged in the usual canonical layout,
-// once for all T tiles; one thread issues the tap's MMAs of every tile into
+// the next plane at LBO = 16 R bytes.  The weights (all output channels,
+// N = NP padded to 16) are staged beside the input in the usual canonical
+// layout, once for all T tiles, TG taps at a time (all nine where shared
+// memory allows); one thread issues the group's MMAs of every tile into
 // its TMEM accumulator and commits them to an mbarrier that every thread
-// waits on (bounded) before the weights are refilled.  Each warp reads its 32 rows back (tcgen05.ld),
-// adds the bias, applies ReLU and stores the interior pixels in f32.
+// waits on (bounded).  Each warp reads its 32 rows back (tcgen05.ld), adds
+// the bias, applies ReLU and stores the interior pixels in f32.
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;
 constexpr int TC_MAX_SMEM = 200 * 1024;
 
@@ -295,18 +296,19 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// Dynamic shared memory of the tensor-core convolution (bytes), T tiles.
-__host__ __device__ inline size_t tc_smem_bytes(int ci, int w, int np, int T) {
+// Dynamic shared memory of the tensor-core convolution (bytes), T tiles:
+// the staged input planes and the weights of TG taps.
+__host__ __device__ inline size_t tc_smem_bytes(int ci, int w, int np, int T, int TG) {
   const size_t R = 128 * (size_t)T + 2 * (size_t)(w + 3);
   const size_t G = 2 * (size_t)((ci + 15) / 16);
-  return G * R * 16 + (G / 2) * (size_t)np * 32;
+  return G * R * 16 + (size_t)TG * (G / 2) * (size_t)np * 32;
 }
 
 template <int NP>
 __global__ void __launch_bounds__(128)
 k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __restrict__ out, int64_t out_ns,
              int co_n, int H, int W, const float* __restrict__ wt, const float* __restrict__ bias, int relu,
-             int T) {
+             int T, int TG) {
   constexpr uint32_t NCOL = NP <= 32 ? 32 : (NP <= 64 ? 64 : 128);
   // TMEM columns: one NCOL accumulator per tile, allocated as a power of two.
   const uint32_t ncols = (uint32_t)T * NCOL <= 32u ? 32u : ((uint32_t)T * NCOL <= 64u ? 64u :
@@ -314,7 +316,7 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
   extern __shared__ __align__(1024) unsigned char smem[];
   const int P = W + 2, R = 128 * T + 2 * (P + 1), G = 2 * ((ci_n + 15) / 16), S = G / 2;
   uint4* sa = reinterpret_cast<uint4*>(smem);  // G planes x R rows of 16 B
-  uint4* sb = sa + (size_t)G * R;               // S K steps x (NP / 8) x 2 core matrices x 8 rows
+  uint4* sb = sa + (size_t)G * R;               // TG taps x S K steps x (NP / 8) x 2 core matrices x 8 rows
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_base;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -353,32 +355,42 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NP >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
   const uint32_t lbo_a = (uint32_t)R * 16u;
-  for (int tap = 0; tap < 9; ++tap) {
-    // weights of this tap: B[co][16 s + kk] = w[co][16 s + kk][tap]
-    for (int idx = t; idx < S * NP * 2; idx += 128) {
-      const int s = idx / (NP * 2), rem = idx - s * NP * 2, co = rem >> 1, h = rem & 1;
+  const int per_tap = S * NP * 2;  // uint4 rows of one tap's weights
+  // Taps in groups of TG (all nine where shared memory allows): the group's
+  // weights B[co][16 s + kk] = w[co][16 s + kk][tap] are staged, one thread
+  // issues the group's MMAs of every tile into its TMEM accumulator and
+  // commits them to an mbarrier that every thread waits on (bounded) before
+  // the next group's weights overwrite these.
+  for (int tap0 = 0, ph = 0; tap0 < 9; tap0 += TG, ++ph) {
+    const int ntap = min(TG, 9 - tap0);
+    for (int idx = t; idx < ntap * per_tap; idx += 128) {
+      const int k = idx / per_tap, r0 = idx - k * per_tap, tap = tap0 + k;
+      const int s = r0 / (NP * 2), rem = r0 - s * NP * 2, co = rem >> 1, h = rem & 1;
       float v[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int ci = s * 16 + h * 8 + j;
         v[j] = (co < co_n && ci < ci_n) ? wt[((int64_t)co * ci_n + ci) * 9 + tap] : 0.0f;
       }
-      sb[(s * (NP / 4) + (co >> 3) * 2 + h) * 8 + (co & 7)] =
+      sb[k * per_tap + (s * (NP / 4) + (co >> 3) * 2 + h) * 8 + (co & 7)] =
           make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (t == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int row0 = (P + 1) + (tap / 3 - 1) * P + (tap % 3 - 1);
-      for (int m = 0; m < T; ++m) {  // tile m: rows 128 m.. of the window, accumulator columns m NCOL..
-        for (int s = 0; s < S; ++s) {
-          const uint64_t da = umma_desc(smem_addr(sa + (size_t)(2 * s) * R + row0 + 128 * m), lbo_a, 128u);
-          const uint64_t db = umma_desc(smem_addr(sb + (size_t)s * NP * 2), 128u, 256u);
-          const uint32_t acc = (tap > 0 || s > 0) ? 1u : 0u;
-          asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                       " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-                       ::"r"(tmem + (uint32_t)m * NCOL), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+      for (int k = 0; k < ntap; ++k) {
+        const int tap = tap0 + k;
+        const int row0 = (P + 1) + (tap / 3 - 1) * P + (tap % 3 - 1);
+        for (int m = 0; m < T; ++m) {  // tile m: rows 128 m.. of the window, accumulator columns m NCOL..
+          for (int s = 0; s < S; ++s) {
+            const uint64_t da = umma_desc(smem_addr(sa + (size_t)(2 * s) * R + row0 + 128 * m), lbo_a, 128u);
+            const uint64_t db = umma_desc(smem_addr(sb + (size_t)k * per_tap + (size_t)s * NP * 2), 128u, 256u);
+            const uint32_t acc = (tap > 0 || s > 0) ? 1u : 0u;
+            asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                         " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                         ::"r"(tmem + (uint32_t)m * NCOL), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+          }
         }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
@@ -387,7 +399,7 @@ k_conv3x3_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, float* __res
     uint32_t done = 0;
     for (uint32_t it = 0; it < TC_WAIT_LIMIT && !done; ++it)
       asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                   : "=r"(done) : "r"(smem_addr(&bar)), "r"((uint32_t)(tap & 1)) : "memory");
+                   : "=r"(done) : "r"(smem_addr(&bar)), "r"((uint32_t)(ph & 1)) : "memory");
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
   // epilogue: TMEM row i of accumulator m = output position q0 + 128 m + i
@@ -639,8 +651,12 @@ cudaError_t launch_tc(const float* in, int64_t in_ns, int ci, float* out, int64_
   const int64_t span = (int64_t)(h - 1) * P + w;  // output positions from the first to the last pixel
   const int64_t tiles = (span + 127) / 128;
   int T = (int)std::max<int64_t>(1, std::min<int64_t>({4, tiles, tiles * n / (4 * 148)}));
-  while (T > 1 && tc_smem_bytes(ci, w, NP, T) > (size_t)TC_MAX_SMEM) --T;
-  const size_t smem = tc_smem_bytes(ci, w, NP, T);
+  // All nine taps' weights at once where they fit (one MMA burst, one
+  // wait), else groups of three, else one tap at a time.
+  int TG = 9;
+  while (T > 1 && tc_smem_bytes(ci, w, NP, T, TG) > (size_t)TC_MAX_SMEM) --T;
+  while (TG > 1 && tc_smem_bytes(ci, w, NP, T, TG) > (size_t)TC_MAX_SMEM) TG = TG > 3 ? 3 : 1;
+  const size_t smem = tc_smem_bytes(ci, w, NP, T, TG);
   if (smem > (size_t)TC_MAX_SMEM) return cudaErrorInvalidValue;
   static bool attr = false;  // per instantiation; the same limit on every device
   if (!attr) {
@@ -649,7 +665,7 @@ cudaError_t launch_tc(const float* in, int64_t in_ns, int ci, float* out, int64_
     attr = true;
   }
   const dim3 grid((unsigned)((tiles + T - 1) / T), n);
-  k_conv3x3_tc<NP><<<grid, 128, smem, s>>>(in, in_ns, ci, out, out_ns, co, h, w, weight, bias, relu ? 1 : 0, T);
+  k_conv3x3_tc<NP><<<grid, 128, smem, s>>>(in, in_ns, ci, out, out_ns, co, h, w, weight, bias, relu ? 1 : 0, T, TG);
   return cudaGetLastError();
 }
 

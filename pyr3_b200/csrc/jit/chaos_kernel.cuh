@@ -1015,6 +1015,7 @@ chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ W
     mbar_init(&wbar);
   for (u32 i = t; i < (u32)(MAXRANK * NXF); i += WB) pst[i] = A.pick_start[i];
   if (blockIdx.x == 0 && t < (u32)NXF && W.mode != 2u) W.cnt[W.zero_cnt * NXF + t] = 0u;
+  if (t < (u32)NXF) scnt[t] = 0u;  // sort counts, first used after the iteration
   if (W.mode != 0u && warp == 0) {
     // This block's work item: chunk c of region k, regions in xform order.
     const u32 c = lane < (u32)NXF ? W.cnt[W.rd_cnt * NXF + lane] : 0u;
@@ -1138,8 +1139,6 @@ chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ W
   if (W.mode == 2u) return;
 
   // ---- sort by next xform, reserve region space, write out
-  if (t < (u32)NXF) scnt[t] = 0u;
-  __syncthreads();
   u32 rank = 0u;
   if (alive) {
     rank = atomicAdd(&scnt[nfn], 1u);
@@ -1179,10 +1178,11 @@ chaos_wave_kernel(const __grid_constant__ ChaosArgs A, const __grid_constant__ W
     // population reads the records back.
     u64 pol;
     asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    u32* dst = wave_field(W, W.wr_buf, kk, 0) + g;
 #pragma unroll 4
-    for (u32 f = 0; f < (u32)WRNG; ++f) st_keep(wave_field(W, W.wr_buf, kk, f) + g, srng[f * WB + src], pol);
+    for (u32 f = 0; f < (u32)WRNG; ++f, dst += W.cap) st_keep(dst, srng[f * WB + src], pol);
 #pragma unroll
-    for (u32 f = 0; f < 6u; ++f) st_keep(wave_field(W, W.wr_buf, kk, WRNG + f) + g, sfs[f * WB + src], pol);
+    for (u32 f = 0; f < 6u; ++f, dst += W.cap) st_keep(dst, sfs[f * WB + src], pol);
   }
 }
 #endif  // WAVE
