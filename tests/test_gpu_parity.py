@@ -857,6 +857,43 @@ def test_wave_kernel_pool_fits_half_of_l2():
     r.destroy()
 
 
+def test_headline_full_size_default_path():
+    """The bench's workload at full size through the default (autotuned)
+    path: 1920x1080 oversample 2, 500 spp, 1.0368e9 samples.  Checks that
+    hold at any size: every sample is counted; the count channel holds 255
+    per in-canvas splat (every xform is opaque) and no cell saturates; the
+    in-canvas share of the samples is that of a 480x270 render of the same
+    view (scale W / 4), within 0.5 % of the samples, since the resolution
+    does not move the attractor; the present is a non-empty image."""
+    import copy
+
+    g = workloads.headline_1080p()
+    W, H = g.size
+    walkers, iters, total = R.compute_dispatch(g.quality, W, H)
+    assert total == 1_036_800_000
+    r = R.create_renderer(W, H, g.oversample)
+    r.reset(g)
+    r.iterate(g, seed=21, walkers=walkers, iters_per_walker=iters)
+    s, n_in = r.counters()
+    assert s == total
+    hist, _, _ = r.read_histogram()
+    assert int(hist.max()) < 0xFFFFFFFF
+    assert int(hist.reshape(-1, 4)[:, 3].astype(np.uint64).sum()) == 255 * n_in
+    img = r.present(g, total)
+    r.destroy()
+    assert img.shape == (H, W, 4) and int(img[..., :3].max()) > 0
+    g2 = copy.deepcopy(g)
+    g2.size, g2.scale = (480, 270), 480 / 4
+    w2, it2, t2 = R.compute_dispatch(g2.quality, 480, 270)
+    r2 = R.create_renderer(480, 270, g2.oversample)
+    r2.reset(g2)
+    r2.iterate(g2, seed=22, walkers=w2, iters_per_walker=it2)
+    s2, n2 = r2.counters()
+    r2.destroy()
+    assert s2 == t2
+    assert abs(n_in / s - n2 / s2) < 0.005, (n_in / s, n2 / s2)
+
+
 def test_queue_kernel_refills_walker_slots():
     """More walkers than the resident slots (exact-walkers mode), so slots
     are refilled as walkers finish: every walker runs exactly its
