@@ -486,43 +486,32 @@ k_wgrad_tc(const float* __restrict__ in, int64_t in_ns, int ci_n, const float* _
   }
   int phase = 0;
   for (int qs = q_begin; qs < q_end; qs += WT_KC, ++phase) {
-    // A rows: output channel co (128 rows), 8 positions per 16-byte row.
-    // Rows past co_n stay zero (written once, below); the padded-grid
-    // coordinates of a group's first position are divided out once and
-    // stepped along the row.
-    for (int idx = t; idx < co_n * (WT_KC / 8); idx += 128) {
-      const int co = idx >> 3, g = idx & 7;
-      const int q0 = qs + g * 8;
-      int yy = q0 / P, xx = q0 - yy * P;
-      const float* src = dn + co * hw;
-      float v[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        v[j] = (q0 + j < q_end && yy >= 1 && yy <= H && xx >= 1 && xx <= W) ? src[(int64_t)(yy - 1) * W + (xx - 1)]
-                                                                          : 0.0f;
-        if (++xx == P) { xx = 0; ++yy; }
+    // A rows (output channel co: dout, zero at padding positions and past
+    // the chunk) and B rows (input channel ci: the input at the position
+    // shifted by the tap), as bf16 in the operands' 16-byte rows of 8
+    // positions.  Each thread stages one position of the step, p = t mod 64,
+    // for every second channel, so the lanes of a warp read 32 consecutive
+    // positions of one channel: one coalesced request per load.  A rows past
+    // co_n stay zero (written once, above).
+    {
+      const int p = t & (WT_KC - 1);
+      const int q = qs + p, qi = q + d;  // qi >= 0: q >= P + 1, d >= -(P + 1)
+      const int yy = q / P, xx = q - yy * P;
+      const int yi = qi / P, xi = qi - yi * P;
+      const bool in_a = q < q_end && yy >= 1 && yy <= H && xx >= 1 && xx <= W;
+      const bool in_b = q < q_end && yi >= 1 && yi <= H && xi >= 1 && xi <= W;
+      const int64_t off_a = (int64_t)(yy - 1) * W + (xx - 1), off_b = (int64_t)(yi - 1) * W + (xi - 1);
+      const int g = p >> 3, s = g >> 1, h = g & 1, e = p & 7;
+      unsigned short* sa16 = reinterpret_cast<unsigned short*>(sa);
+      unsigned short* sb16 = reinterpret_cast<unsigned short*>(sb);
+      for (int co = t / WT_KC; co < co_n; co += 128 / WT_KC) {
+        const float v = in_a ? dn[co * hw + off_a] : 0.0f;
+        sa16[((s * 32 + (co >> 3) * 2 + h) * 8 + (co & 7)) * 8 + e] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
       }
-      const int s = g >> 1, h = g & 1;
-      sa[(s * 32 + (co >> 3) * 2 + h) * 8 + (co & 7)] =
-          make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
-    }
-    // B rows: input channel ci, the positions shifted by the tap
-    for (int idx = t; idx < NP * (WT_KC / 8); idx += 128) {
-      const int ci = idx >> 3, g = idx & 7;
-      const int q0 = qs + g * 8, qi0 = q0 + d;
-      int yy = qi0 / P, xx = qi0 - yy * P;
-      const float* src = ip + ci * hw;
-      float v[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        v[j] = (ci < ci_n && q0 + j < q_end && yy >= 1 && yy <= H && xx >= 1 && xx <= W)
-                   ? src[(int64_t)(yy - 1) * W + (xx - 1)]
-                   : 0.0f;
-        if (++xx == P) { xx = 0; ++yy; }
+      for (int ci = t / WT_KC; ci < NP; ci += 128 / WT_KC) {
+        const float v = (in_b && ci < ci_n) ? ip[ci * hw + off_b] : 0.0f;
+        sb16[((s * (NP / 4) + (ci >> 3) * 2 + h) * 8 + (ci & 7)) * 8 + e] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
       }
-      const int s = g >> 1, h = g & 1;
-      sb[(s * (NP / 4) + (ci >> 3) * 2 + h) * 8 + (ci & 7)] =
-          make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
