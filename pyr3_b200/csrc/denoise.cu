@@ -157,20 +157,17 @@ __global__ void k_flip(const float* __restrict__ w, int co_n, int ci_n, float* _
   wt[((int64_t)ci * co_n + co) * 9 + (8 - k)] = w[i];
 }
 
-// Element i of c channels x hw pixels of image n lives at n * ns + i.
-__global__ void k_relu_mask(float* g, int64_t g_ns, const float* __restrict__ y, int64_t y_ns,
-                            int64_t per, int n_img) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= per * n_img) return;
-  const int64_t n = i / per, r = i % per;
+// Element r of c channels x hw pixels of image n lives at n * ns + r; the
+// grid's y is the image.
+__global__ void k_relu_mask(float* g, int64_t g_ns, const float* __restrict__ y, int64_t y_ns, int64_t per) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, n = blockIdx.y;
+  if (r >= per) return;
   if (!(y[n * y_ns + r] > 0.0f)) g[n * g_ns + r] = 0.0f;
 }
 
-__global__ void k_add(float* y, int64_t y_ns, const float* __restrict__ x, int64_t x_ns, int64_t per,
-                      int n_img) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= per * n_img) return;
-  const int64_t n = i / per, r = i % per;
+__global__ void k_add(float* y, int64_t y_ns, const float* __restrict__ x, int64_t x_ns, int64_t per) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, n = blockIdx.y;
+  if (r >= per) return;
   y[n * y_ns + r] += x[n * x_ns + r];
 }
 
@@ -564,7 +561,16 @@ k_bias_part(const float* __restrict__ dout, int64_t dout_ns, int co_n, int n_img
   const int co = blockIdx.x, s = blockIdx.y;
   const int64_t P = hw * n_img, p0 = P * s / kWgChunks, p1 = P * (s + 1) / kWgChunks;
   float a = 0.0f;
-  for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) a += dout[(p / hw) * dout_ns + co * hw + p % hw];
+  // position p = image img, pixel off; divided once, then stepped
+  int64_t p = p0 + threadIdx.x, img = p / hw, off = p - img * hw;
+  for (; p < p1; p += blockDim.x) {
+    a += dout[img * dout_ns + co * hw + off];
+    off += blockDim.x;
+    while (off >= hw) {
+      off -= hw;
+      ++img;
+    }
+  }
   __shared__ float red[8];
   for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
@@ -690,14 +696,18 @@ cudaError_t dn_flip_weights(const float* w, int co, int ci, float* wt, cudaStrea
 cudaError_t dn_relu_mask(float* g, int64_t g_ns, const float* y, int64_t y_ns, int c, int n, int hw,
                          cudaStream_t s) {
   const int64_t per = (int64_t)c * hw;
-  k_relu_mask<<<blocks_for(per * n), 256, 0, s>>>(g, g_ns, y, y_ns, per, n);
+  for (int n0 = 0; n0 < n && per > 0; n0 += 65535)  // grid y: up to 65535 images per launch
+    k_relu_mask<<<dim3(blocks_for(per), std::min(65535, n - n0)), 256, 0, s>>>(g + n0 * g_ns, g_ns, y + n0 * y_ns,
+                                                                             y_ns, per);
   return cudaGetLastError();
 }
 
 cudaError_t dn_add(float* y, int64_t y_ns, const float* x, int64_t x_ns, int c, int n, int hw,
                    cudaStream_t s) {
   const int64_t per = (int64_t)c * hw;
-  k_add<<<blocks_for(per * n), 256, 0, s>>>(y, y_ns, x, x_ns, per, n);
+  for (int n0 = 0; n0 < n && per > 0; n0 += 65535)  // grid y: up to 65535 images per launch
+    k_add<<<dim3(blocks_for(per), std::min(65535, n - n0)), 256, 0, s>>>(y + n0 * y_ns, y_ns, x + n0 * x_ns, x_ns,
+                                                                       per);
   return cudaGetLastError();
 }
 
