@@ -184,7 +184,7 @@ int device_sms(int dev) {
 
 int g_l2_bytes = 0;
 
-// L2 size in bytes (126 MiB on B200).
+// L2 size in bytes (about 126.5 MiB on B200).
 uint64_t device_l2(int dev) {
   if (g_l2_bytes == 0) cudaDeviceGetAttribute(&g_l2_bytes, cudaDevAttrL2CacheSize, dev);
   return g_l2_bytes > 0 ? (uint64_t)g_l2_bytes : (126ull << 20);

@@ -830,7 +830,7 @@ def test_wave_kernel_pool_split():
 
 def test_wave_kernel_pool_fits_half_of_l2():
     """A default wave launch of 10^9 samples takes the walkers whose records
-    (196 B each) fill half of L2 -- 336,896 on B200, ~2,968 iterations each,
+    (196 B each) fill half of L2 -- 337,920 on B200, ~2,959 iterations each,
     where 2,000-iteration walkers would be 500,000 -- so the launch count (a
     seeding launch, one per iteration, a last launch, for each of the two
     populations) shows more than 2,500 iterations.  Every sample is counted

@@ -68,7 +68,8 @@ def _check(name, g, dev_hist, dev_img, ref1, ref2, W, H, os_, samples):
 
 
 # Iterations per walker of the bench's headline launch: 1.0368e9 samples on
-# 336,896 walkers (the wave pool whose records fill half of L2).
+# ~338,000 walkers (the wave pool whose records fill half of L2: 337,920 on
+# B200, ~3,068 iterations each; 3,077 is within 0.3 % of that).
 BENCH_ITERS = 3077
 
 
@@ -81,7 +82,7 @@ def test_headline_genome_matches_reference(pool, W, H, spp):
     reference's computeDispatch split (1024 walkers):
 
     * 480x270 at the bench's 500 spp (6.48e7 samples), with walkers of 3,077
-      iterations (the bench's iterations per walker: 336,896 walkers at full
+      iterations (about the bench's iterations per walker: ~338,000 walkers at full
       size), and with the small-launch pool (~279k walkers of ~232
       iterations, where the 200-iteration burn-in weighs most).  At 500 spp
       two reference seeds are themselves only ~32.6 dB apart, so the image
